@@ -1,0 +1,222 @@
+"""CPU tests of the oracle itself: pinned against the reference's stored
+streams, and the reference crate's own unit tests restated
+(`crates/fqxv-rans/src/lib.rs:261-604`, `model.rs:266-392`)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+
+# --- the pin: stored bytes from the reference's container fixtures --------
+
+def test_golden_streams_decode_and_reencode_identically(orc, golden):
+    assert len(golden) == 32
+    for meta, stream in golden:
+        dec = orc.decode(stream)
+        assert len(dec) == meta["n"]
+        assert orc.encode(dec, stream[0]) == stream, meta["stream"]
+
+
+def test_golden_streams_simd_paths_agree(orc, golden):
+    if orc.simd_level() < 1:
+        pytest.skip("no AVX2 on this host")
+    levels = ["avx2"] + (["avx512"] if orc.simd_level() >= 2 else [])
+    for _, stream in golden:
+        dec = orc.decode(stream)
+        for p in levels:
+            assert orc.decode(stream, path=p) == dec
+            assert orc.encode(dec, 0, path=p) == stream
+
+
+# --- model.rs tests -----------------------------------------------------------
+
+def _check_sum(orc, counts):
+    f = orc.normalize(counts).astype(np.int64)
+    assert f.sum() == 4096
+    c = np.asarray(counts)
+    assert np.all(f[c > 0] >= 1)
+    assert np.all(f[c == 0] == 0)
+    return f
+
+
+def test_normalize_single_symbol(orc):
+    c = np.zeros(256, np.uint32)
+    c[65] = 100
+    assert _check_sum(orc, c)[65] == 4096
+
+
+def test_normalize_uniform_skewed_two_symbols(orc):
+    _check_sum(orc, np.full(256, 7, np.uint32))
+    c = np.ones(256, np.uint32)
+    c[0] = 10_000_000
+    _check_sum(orc, c)
+    c = np.zeros(256, np.uint32)
+    c[0], c[255] = 3, 1
+    _check_sum(orc, c)
+
+
+def test_normalize_random_histograms(orc):
+    rng = np.random.default_rng(7)
+    for _ in range(300):
+        k = int(rng.integers(1, 257))
+        c = np.zeros(256, np.uint32)
+        idx = rng.choice(256, k, replace=False)
+        c[idx] = rng.integers(1, 1 << int(rng.integers(1, 24)), k)
+        _check_sum(orc, c)
+
+
+def test_reciprocal_and_magic_match_division(orc):
+    L = orc.lib()
+    L.orc_check_apply_sweep.restype = ctypes.c_size_t
+    assert L.orc_check_apply_sweep() == 0
+
+
+def test_validate_rejects_malformed_tables(orc):
+    assert orc.validate_freqs(np.zeros(256, np.uint16)) == 4
+    over = np.zeros(256, np.uint16)
+    over[0] = 4097
+    assert orc.validate_freqs(over) == 3
+    spread = np.zeros(256, np.uint16)
+    spread[0] = spread[1] = 3000
+    assert orc.validate_freqs(spread) == 3
+    ok = np.zeros(256, np.uint16)
+    ok[0] = 4096
+    assert orc.validate_freqs(ok) == 0
+
+
+# --- lib.rs tests -------------------------------------------------------------
+
+def _roundtrip(orc, data):
+    for order in (0, 1):
+        enc = orc.encode(data, order)
+        assert orc.decode(enc) == bytes(data), (order, len(data))
+
+
+def test_roundtrip_empty_single_allsame(orc):
+    _roundtrip(orc, b"")
+    _roundtrip(orc, b"Q")
+    _roundtrip(orc, b"A" * 1000)
+    assert orc.encode(b"", 0) == bytes(9)
+    assert orc.encode(b"", 1) == b"\x01" + bytes(8)
+
+
+def test_roundtrip_short_and_odd_lengths(orc):
+    for n in [1, 2, 31, 32, 33, 63, 64, 65, 100]:
+        _roundtrip(orc, bytes((i * 7 + 3) & 0xFF for i in range(n)))
+
+
+def test_roundtrip_full_alphabet(orc):
+    _roundtrip(orc, bytes(i & 0xFF for i in range(10_000)))
+
+
+def test_compresses_skewed_data(orc):
+    data = bytes((ord("I") - (i % 8) * (i % 3 == 0)) for i in range(50_000))
+    enc = orc.encode(data, 0)
+    assert len(enc) < len(data) // 2
+    assert orc.decode(enc) == data
+
+
+def test_order1_beats_order0_on_correlated_data(orc):
+    x = 0
+    data = bytearray()
+    for i in range(100_000):
+        x = (x + (i % 4)) & 0xFF
+        data.append(ord("A") + (x % 4))
+    assert len(orc.encode(data, 1)) < len(orc.encode(data, 0))
+
+
+def test_roundtrip_random_small_alphabet_and_arbitrary(orc):
+    rng = np.random.default_rng(1)
+    for _ in range(40):
+        n = int(rng.integers(0, 2000))
+        _roundtrip(orc, rng.integers(0, 6, n).astype(np.uint8).tobytes())
+        _roundtrip(orc, rng.integers(0, 256, n).astype(np.uint8).tobytes())
+
+
+def test_simd_matches_scalar(orc):
+    if orc.simd_level() < 1:
+        pytest.skip("no AVX2 on this host")
+    levels = ["avx2"] + (["avx512"] if orc.simd_level() >= 2 else [])
+    rng = np.random.default_rng(2)
+    cases = [rng.integers(0, 40, int(rng.integers(0, 5000))).astype(np.uint8).tobytes() for _ in range(30)]
+    cases += [bytes((i * 131 % 251) for i in range(n)) for n in [0, 1, 5, 31, 32, 33, 64, 65, 1000, 100_003]]
+    # lib.rs:439-447: a dominant (freq > 2048) symbol, a single symbol, a 2-symbol skew
+    cases += [b"A" * 60_000 + bytes(ord("B") + (i % 20) for i in range(4000)), b"Q" * 40_000,
+              bytes(ord("!") + 7 * (i % 3 == 0) for i in range(80_000))]
+    for data in cases:
+        ref = orc.encode(data, 0)
+        for p in levels:
+            assert orc.encode(data, 0, path=p) == ref
+            assert orc.decode(ref, path=p) == data
+
+
+def test_decode_bounded_rejects_inflated_length(orc):
+    enc = bytearray(orc.encode(b"A" * 64, 0))
+    bomb = bytearray(enc)
+    bomb[1:9] = (1 << 31).to_bytes(8, "little")
+    assert orc.decode_status(bytes(bomb), max_len=1 << 20)[0] == 7
+    assert orc.decode(bytes(enc), max_len=1 << 20) == b"A" * 64
+    assert orc.decode_status(bytes(enc[:1]), max_len=1 << 20)[0] == 1
+
+
+def test_decode_rejects_malformed_freq_table(orc):
+    src = b"\x00" + (1).to_bytes(8, "little")
+    freq = np.zeros(256, np.uint16)
+    freq[0] = 4096 + 100
+    assert orc.decode_status(src + freq.tobytes())[0] == 3
+
+
+def test_decode_rejects_huge_output_length(orc):
+    src = b"\x00" + (2**64 - 1).to_bytes(8, "little")
+    freq = np.zeros(256, np.uint16)
+    freq[0] = 4096
+    src += freq.tobytes() + bytes(4 * 32)
+    assert orc.decode_status(src, cap=1 << 20)[0] == 6
+
+
+def test_decode_error_kinds(orc):
+    assert orc.decode_status(b"")[0] == 1
+    assert orc.decode_status(b"\x05" + (3).to_bytes(8, "little"))[0] == 2
+    assert orc.decode_status(b"\x05" + (0).to_bytes(8, "little")) == (0, b"")  # n == 0 first
+    # order-1 stream whose bitmap lacks context 0: the first symbol fails
+    src = b"\x01" + (4).to_bytes(8, "little") + bytes([0b10]) + bytes(31)
+    freq = np.zeros(256, np.uint16)
+    freq[7] = 4096
+    src += freq.tobytes() + (65536).to_bytes(4, "little") * 32
+    assert orc.decode_status(src)[0] == 5
+    # truncated renorm region
+    enc = orc.encode(bytes(range(40)) * 50, 0)
+    assert orc.decode_status(enc[:-6])[0] == 1
+
+
+def _corrupt(data, rng):
+    data = bytearray(data)
+    for _ in range(int(rng.integers(0, 12))):
+        if data:
+            data[int(rng.integers(0, len(data)))] = int(rng.integers(0, 256))
+    if data and rng.random() < 0.5:
+        i = int(rng.integers(0, len(data)))
+        w = int(rng.integers(1, 9))
+        data[i:i + w] = b"\xff" * len(data[i:i + w])
+    if data and rng.random() < 0.5:
+        data = data[:int(rng.integers(0, len(data)))]
+    return bytes(data)
+
+
+def test_decode_survives_mutation_and_garbage(orc):
+    rng = np.random.default_rng(3)
+    for _ in range(400):
+        data = rng.integers(0, 40, int(rng.integers(0, 2000))).astype(np.uint8).tobytes()
+        enc = orc.encode(data, int(rng.integers(0, 2)))
+        orc.decode_status(_corrupt(enc, rng), max_len=len(data))
+    for _ in range(400):
+        g = bytearray(rng.integers(0, 256, int(rng.integers(0, 256))).astype(np.uint8).tobytes())
+        for tag in (None, 0, 1):
+            b = bytearray(g)
+            if tag is not None:
+                if b:
+                    b[0] = tag
+                else:
+                    b.append(tag)
+            orc.decode_status(bytes(b), max_len=1 << 16)
