@@ -1,0 +1,501 @@
+// C ABI of libfqxv_rans_gpu.so: contexts, device arenas, the batched device
+// API and the reference-shaped single-call host API (include/fqxv_rans_gpu.h).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "rans_internal.cuh"
+
+using namespace fqxv;
+
+namespace {
+
+// Grow-only device buffer. Growth waits for the owning stream first, so a
+// buffer is never freed under a kernel that still reads it.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t want, cudaStream_t s) {
+        if (want <= cap) return cudaSuccess;
+        size_t nc = std::max(want, cap + cap / 2);
+        nc = align_up(nc, 1 << 20);
+        if (p) {
+            cudaStreamSynchronize(s);
+            cudaFree(p);
+            p = nullptr;
+            cap = 0;
+        }
+        cudaError_t e = cudaMalloc(&p, nc);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            e = cudaMalloc(&p, want);
+            if (e != cudaSuccess) {
+                p = nullptr;
+                return e;
+            }
+            nc = want;
+        }
+        cap = nc;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t want) {
+        if (want <= cap) return cudaSuccess;
+        size_t nc = align_up(std::max(want, cap + cap / 2), 1 << 16);
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaHostAlloc(&p, nc, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        cap = nc;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct fqxv_rans_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    // encode
+    DevBuf e_blocks, e_order, e_jobs, e_tbl, e_words, e_hist, e_misc;
+    // decode
+    DevBuf d_streams, d_order, d_tbl, d_misc;
+    // single-call staging
+    DevBuf io_in, io_out;
+    HostBuf h_stage;
+    uint64_t device_bytes() const {
+        const DevBuf *all[] = {&e_blocks, &e_order, &e_jobs, &e_tbl, &e_words, &e_hist, &e_misc,
+                               &d_streams, &d_order, &d_tbl, &d_misc, &io_in, &io_out};
+        uint64_t t = 0;
+        for (auto *b : all) t += b->cap;
+        return t;
+    }
+};
+
+namespace fqxv {
+int sm_count(int device) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 148;
+    return v > 0 ? v : 148;
+}
+}  // namespace fqxv
+
+#define CK(x)                                                          \
+    do {                                                               \
+        cudaError_t e_ = (x);                                          \
+        if (e_ != cudaSuccess) {                                       \
+            cudaGetLastError();                                        \
+            return e_ == cudaErrorMemoryAllocation ? FQXV_RANS_E_OUT_OF_MEMORY \
+                                                   : FQXV_RANS_E_CUDA; \
+        }                                                              \
+    } while (0)
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+uint64_t enc_bound_one(uint64_t n, int order) {
+    if (n == 0) return kHdr;
+    const uint64_t tables = order == FQXV_RANS_ORDER0 ? kO0Tables : kO1Bitmap + 256 * kO1Table;
+    return kHdr + tables + kStatesBytes + 2 * n;
+}
+
+int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks,
+                      size_t nb, int mode, uint8_t *d_dst, uint64_t dst_cap, fqxv_rans_span *out_spans,
+                      int32_t *out_orders, int persistent) {
+    if (mode < FQXV_RANS_ORDER0 || mode > FQXV_RANS_BEST_TIE1) return FQXV_RANS_E_INVALID_ARG;
+    if (nb == 0) return FQXV_RANS_OK;
+    if (nb > (1u << 30)) return FQXV_RANS_E_TOO_LARGE;
+    cudaStream_t s = ctx->stream;
+    const bool o0 = mode != FQXV_RANS_ORDER1, o1 = mode != FQXV_RANS_ORDER0;
+
+    std::vector<EncBlock> hb(nb);
+    uint64_t woff = 0, toff = 0, bound = 0;
+    for (size_t i = 0; i < nb; i++) {
+        EncBlock &B = hb[i];
+        std::memset(&B, 0, sizeof B);
+        B.src_off = blocks[i].offset;
+        B.n = blocks[i].length;
+        B.mode = mode;
+        B.word_off[0] = woff;
+        if (o0) woff += B.n;
+        B.word_off[1] = woff;
+        if (o1) woff += B.n;
+        B.tbl_off = toff;
+        toff += align_up(o1 ? enc_table_bytes(B.n) : kTblUmap, 256);
+        bound += enc_bound_one(B.n, o1 ? FQXV_RANS_ORDER1 : FQXV_RANS_ORDER0);
+    }
+    // Largest blocks first: the model kernel strides over this order and the
+    // encode queue hands jobs out in it (longest-processing-time first).
+    std::vector<uint32_t> ord(nb);
+    std::iota(ord.begin(), ord.end(), 0u);
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return hb[a].n > hb[b].n; });
+    std::vector<EncJob> jobs;
+    jobs.reserve(nb * 2);
+    for (uint32_t b : ord) {
+        if (o1) jobs.push_back({b, 1});
+        if (o0) jobs.push_back({b, 0});
+    }
+    const int model_grid = (int)std::min<size_t>(nb, (size_t)ctx->sms * 2);
+    CK(ctx->e_blocks.ensure(nb * sizeof(EncBlock), s));
+    CK(ctx->e_order.ensure(nb * sizeof(uint32_t), s));
+    CK(ctx->e_jobs.ensure(jobs.size() * sizeof(EncJob), s));
+    CK(ctx->e_tbl.ensure(std::max<uint64_t>(toff, 256), s));
+    CK(ctx->e_words.ensure(std::max<uint64_t>(woff * 2, 16), s));
+    CK(ctx->e_hist.ensure(o1 ? (size_t)model_grid * 65536 * 4 : 256, s));
+    CK(ctx->e_misc.ensure((2 + nb) * 16, s));
+    // Stage descriptors through pinned memory, one copy per array.
+    const size_t szb = nb * sizeof(EncBlock), szo = nb * 4, szj = jobs.size() * sizeof(EncJob);
+    CK(ctx->h_stage.ensure(szb + szo + szj + 64));
+    cudaStreamSynchronize(s);  // the staging buffer may still feed an earlier copy
+    uint8_t *hs = (uint8_t *)ctx->h_stage.p;
+    std::memcpy(hs, hb.data(), szb);
+    std::memcpy(hs + szb, ord.data(), szo);
+    std::memcpy(hs + szb + szo, jobs.data(), szj);
+    CK(cudaMemcpyAsync(ctx->e_blocks.p, hs, szb, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->e_order.p, hs + szb, szo, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->e_jobs.p, hs + szb + szo, szj, cudaMemcpyHostToDevice, s));
+    int *queue = ctx->e_misc.as<int>();
+    uint64_t *total = reinterpret_cast<uint64_t *>(ctx->e_misc.as<uint8_t>() + 16);
+    CK(cudaMemsetAsync(queue, 0, 16, s));
+
+    EncBlock *dB = ctx->e_blocks.as<EncBlock>();
+    const uint32_t *dO = ctx->e_order.as<uint32_t>();
+    const EncJob *dJ = ctx->e_jobs.as<EncJob>();
+    uint8_t *dT = ctx->e_tbl.as<uint8_t>();
+    uint16_t *dW = ctx->e_words.as<uint16_t>();
+    uint32_t *dH = ctx->e_hist.as<uint32_t>();
+    const int run_grid = ctx->sms * 16;
+    if (persistent) {
+        launch_enc_model(d_src, dB, dO, (int)nb, dT, dH, model_grid, s);
+        launch_enc_run(d_src, dB, dJ, (int)jobs.size(), dT, dW, queue, std::min<int>(run_grid, (int)(jobs.size() + 3) / 4), s);
+    } else {
+        // The plain form: every block gets its own launches, one after the other.
+        const int per = (o0 && o1) ? 2 : 1;
+        for (size_t j = 0; j < nb; j++) {
+            CK(cudaMemsetAsync(queue, 0, 4, s));
+            launch_enc_model(d_src, dB, dO + j, 1, dT, dH, 1, s);
+            launch_enc_run(d_src, dB, dJ + j * per, per, dT, dW, queue, 1, s);
+        }
+    }
+    launch_enc_select_scan(dB, (int)nb, total, s);
+    CK(cudaGetLastError());
+    if (bound > dst_cap) {
+        uint64_t tot = 0;
+        CK(cudaMemcpyAsync(&tot, total, 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (tot > dst_cap) return FQXV_RANS_E_DST_TOO_SMALL;
+    }
+    if (persistent) {
+        launch_enc_pack(dB, (int)nb, dT, dW, d_dst, (int)std::min<size_t>(nb, (size_t)ctx->sms * 8), s);
+    } else {
+        for (size_t j = 0; j < nb; j++) launch_enc_pack(dB + j, 1, dT, dW, d_dst, 1, s);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hs, dB, szb, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const EncBlock *rb = reinterpret_cast<const EncBlock *>(hs);
+    for (size_t i = 0; i < nb; i++) {
+        out_spans[i].offset = rb[i].out_off;
+        out_spans[i].length = rb[i].out_size[rb[i].chosen];
+        if (out_orders) out_orders[i] = rb[i].chosen;
+    }
+    return FQXV_RANS_OK;
+}
+
+int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks, size_t nb,
+                      uint64_t max_len, uint8_t *d_dst, const fqxv_rans_span *out_spans, uint64_t *out_lens,
+                      int32_t *status, int persistent) {
+    if (nb == 0) return FQXV_RANS_OK;
+    if (nb > (1u << 30)) return FQXV_RANS_E_TOO_LARGE;
+    cudaStream_t s = ctx->stream;
+    std::vector<DecStream> hs(nb);
+    uint64_t toff = 0;
+    for (size_t i = 0; i < nb; i++) {
+        DecStream &S = hs[i];
+        std::memset(&S, 0, sizeof S);
+        S.src_off = blocks[i].offset;
+        S.src_len = blocks[i].length;
+        S.dst_off = out_spans[i].offset;
+        S.dst_cap = out_spans[i].length;
+        S.max_len = max_len;
+        S.tbl_off = toff;
+        toff += align_up(dec_table_bytes(S.src_len), 256);
+    }
+    std::vector<uint32_t> ord(nb);
+    std::iota(ord.begin(), ord.end(), 0u);
+    std::stable_sort(ord.begin(), ord.end(),
+                     [&](uint32_t a, uint32_t b) { return hs[a].dst_cap > hs[b].dst_cap; });
+    CK(ctx->d_streams.ensure(nb * sizeof(DecStream), s));
+    CK(ctx->d_order.ensure(nb * 4, s));
+    CK(ctx->d_tbl.ensure(std::max<uint64_t>(toff, 256), s));
+    CK(ctx->d_misc.ensure(256, s));
+    const size_t szs = nb * sizeof(DecStream), szo = nb * 4;
+    CK(ctx->h_stage.ensure(szs + szo + 64));
+    cudaStreamSynchronize(s);
+    uint8_t *hst = (uint8_t *)ctx->h_stage.p;
+    std::memcpy(hst, hs.data(), szs);
+    std::memcpy(hst + szs, ord.data(), szo);
+    CK(cudaMemcpyAsync(ctx->d_streams.p, hst, szs, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->d_order.p, hst + szs, szo, cudaMemcpyHostToDevice, s));
+    int *queue = ctx->d_misc.as<int>();
+    CK(cudaMemsetAsync(queue, 0, 16, s));
+    DecStream *dS = ctx->d_streams.as<DecStream>();
+    const uint32_t *dO = ctx->d_order.as<uint32_t>();
+    uint8_t *dT = ctx->d_tbl.as<uint8_t>();
+    if (persistent) {
+        launch_dec_parse(d_src, dS, (int)nb, dT, (int)std::min<size_t>(nb, (size_t)ctx->sms * 8), s);
+        launch_dec_run(d_src, dS, dO, (int)nb, dT, d_dst, queue,
+                       (int)std::min<size_t>((nb + 3) / 4, (size_t)ctx->sms * 16), s);
+    } else {
+        for (size_t j = 0; j < nb; j++) {
+            CK(cudaMemsetAsync(queue, 0, 4, s));
+            launch_dec_parse(d_src, dS + ord[j], 1, dT, 1, s);
+            launch_dec_run(d_src, dS, dO + j, 1, dT, d_dst, queue, 1, s);
+        }
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hst, dS, szs, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const DecStream *rs = reinterpret_cast<const DecStream *>(hst);
+    int first = FQXV_RANS_OK;
+    for (size_t i = 0; i < nb; i++) {
+        if (status) status[i] = rs[i].status;
+        if (out_lens) out_lens[i] = rs[i].status == FQXV_RANS_OK ? rs[i].n : 0;
+        if (rs[i].status != FQXV_RANS_OK && first == FQXV_RANS_OK) first = rs[i].status;
+    }
+    return first;
+}
+
+// One default context per device for the single-call API.
+std::mutex g_default_mu;
+fqxv_rans_ctx *g_default[64];
+
+int default_ctx(fqxv_rans_ctx **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return FQXV_RANS_E_NO_DEVICE;
+    }
+    if (dev < 0 || dev >= 64) return FQXV_RANS_E_NO_DEVICE;
+    std::lock_guard<std::mutex> g(g_default_mu);
+    if (!g_default[dev]) {
+        const int st = fqxv_rans_ctx_create(dev, &g_default[dev]);
+        if (st != FQXV_RANS_OK) return st;
+    }
+    *out = g_default[dev];
+    return FQXV_RANS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fqxv_rans_status_message(int status) {
+    switch (status) {
+        case FQXV_RANS_OK: return "ok";
+        case FQXV_RANS_E_TRUNCATED: return "truncated stream";
+        case FQXV_RANS_E_UNKNOWN_ORDER: return "unknown order tag";
+        case FQXV_RANS_E_FREQ_EXCEEDS: return "rANS freq table exceeds TOTFREQ";
+        case FQXV_RANS_E_FREQ_SUM: return "rANS freq table does not sum to TOTFREQ";
+        case FQXV_RANS_E_ABSENT_CONTEXT: return "symbol references absent context";
+        case FQXV_RANS_E_ALLOC: return "rANS output length too large to allocate";
+        case FQXV_RANS_E_BOUND: return "rANS output length exceeds caller bound";
+        case FQXV_RANS_E_TRUNCATED_RENORM: return "truncated renorm stream";
+        case FQXV_RANS_E_INVALID_ARG: return "invalid argument";
+        case FQXV_RANS_E_DST_TOO_SMALL: return "destination buffer too small";
+        case FQXV_RANS_E_CUDA: return "CUDA error";
+        case FQXV_RANS_E_NO_DEVICE: return "no CUDA device";
+        case FQXV_RANS_E_OUT_OF_MEMORY: return "device out of memory";
+        case FQXV_RANS_E_TIMEOUT: return "device wait timed out";
+        case FQXV_RANS_E_TOO_LARGE: return "request too large";
+        default: return "unknown status";
+    }
+}
+
+const char *fqxv_rans_version(void) { return "fqxv-rans-b200 0.1.0 (sm_100a)"; }
+
+size_t fqxv_rans_encode_bound(size_t n, int order) {
+    return (size_t)enc_bound_one(n, order == FQXV_RANS_ORDER0 ? FQXV_RANS_ORDER0 : FQXV_RANS_ORDER1);
+}
+
+int fqxv_rans_ctx_create(int device, fqxv_rans_ctx **out) {
+    if (!out) return FQXV_RANS_E_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return FQXV_RANS_E_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return FQXV_RANS_E_INVALID_ARG;
+    DeviceGuard g(device);
+    auto *c = new fqxv_rans_ctx();
+    c->device = device;
+    c->sms = sm_count(device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return FQXV_RANS_E_CUDA;
+    }
+    *out = c;
+    return FQXV_RANS_OK;
+}
+
+void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
+    if (!ctx) return;
+    DeviceGuard g(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    DevBuf *all[] = {&ctx->e_blocks, &ctx->e_order, &ctx->e_jobs, &ctx->e_tbl, &ctx->e_words,
+                     &ctx->e_hist, &ctx->e_misc, &ctx->d_streams, &ctx->d_order, &ctx->d_tbl,
+                     &ctx->d_misc, &ctx->io_in, &ctx->io_out};
+    for (auto *b : all) b->release();
+    ctx->h_stage.release();
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+void *fqxv_rans_ctx_stream(fqxv_rans_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+uint64_t fqxv_rans_ctx_device_bytes(fqxv_rans_ctx *ctx) { return ctx ? ctx->device_bytes() : 0; }
+
+uint64_t fqxv_rans_encode_batch_bound(const fqxv_rans_span *blocks, size_t nblocks, int order) {
+    uint64_t t = 0;
+    for (size_t i = 0; i < nblocks; i++) t += fqxv_rans_encode_bound(blocks[i].length, order);
+    return t;
+}
+
+int fqxv_rans_encode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks,
+                           size_t nblocks, int order, uint8_t *d_dst, uint64_t dst_cap,
+                           fqxv_rans_span *out_spans, int32_t *out_orders, int persistent) {
+    if (!ctx || (nblocks && (!blocks || !out_spans || !d_dst || !d_src))) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    return encode_batch_impl(ctx, d_src, blocks, nblocks, order, d_dst, dst_cap, out_spans, out_orders,
+                             persistent);
+}
+
+int fqxv_rans_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks,
+                           size_t nblocks, uint64_t max_len, uint8_t *d_dst,
+                           const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status,
+                           int persistent) {
+    if (!ctx || (nblocks && (!blocks || !out_spans || !d_src))) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    return decode_batch_impl(ctx, d_src, blocks, nblocks, max_len, d_dst, out_spans, out_lens, status,
+                             persistent);
+}
+
+int fqxv_rans_encode(const uint8_t *src, size_t n, int order, uint8_t *dst, size_t cap, size_t *out_len) {
+    if (!out_len || !dst || (n && !src)) return FQXV_RANS_E_INVALID_ARG;
+    if (order < FQXV_RANS_ORDER0 || order > FQXV_RANS_BEST_TIE1) return FQXV_RANS_E_INVALID_ARG;
+    fqxv_rans_ctx *ctx;
+    int st = default_ctx(&ctx);
+    if (st) return st;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = ctx->stream;
+    const uint64_t bound = enc_bound_one(n, order == FQXV_RANS_ORDER0 ? 0 : 1);
+    CK(ctx->io_in.ensure(std::max<size_t>(n, 16), s));
+    CK(ctx->io_out.ensure(bound, s));
+    if (n) CK(cudaMemcpyAsync(ctx->io_in.p, src, n, cudaMemcpyHostToDevice, s));
+    fqxv_rans_span blk{0, n}, out{0, 0};
+    int32_t chosen = 0;
+    st = encode_batch_impl(ctx, ctx->io_in.as<uint8_t>(), &blk, 1, order, ctx->io_out.as<uint8_t>(), bound, &out,
+                           &chosen, 1);
+    if (st) return st;
+    if (out.length > cap) return FQXV_RANS_E_DST_TOO_SMALL;
+    CK(cudaMemcpyAsync(dst, ctx->io_out.p, out.length, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *out_len = out.length;
+    return FQXV_RANS_OK;
+}
+
+int fqxv_rans_peek_output_len(const uint8_t *src, size_t len, uint64_t *n) {
+    if (!n || (len && !src)) return FQXV_RANS_E_INVALID_ARG;
+    if (len < 9) return FQXV_RANS_E_TRUNCATED;
+    uint64_t v = 0;
+    for (int i = 8; i >= 1; i--) v = (v << 8) | src[i];
+    *n = v;
+    return FQXV_RANS_OK;
+}
+
+int fqxv_rans_decode_bounded(const uint8_t *src, size_t len, size_t max_len, uint8_t *dst, size_t cap,
+                             size_t *out_len) {
+    if (!out_len || (len && !src)) return FQXV_RANS_E_INVALID_ARG;
+    *out_len = 0;
+    uint64_t n = 0;
+    const bool have_n = fqxv_rans_peek_output_len(src, len, &n) == FQXV_RANS_OK;
+    if (have_n && n > (uint64_t)max_len) return FQXV_RANS_E_BOUND;  // lib.rs:227, before decoding
+    fqxv_rans_ctx *ctx;
+    int st = default_ctx(&ctx);
+    if (st) return st;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = ctx->stream;
+    // Output staging only up to what the caller can take; a longer declared
+    // length fails in the parse kernel with FQXV_RANS_E_ALLOC.
+    const uint64_t dev_out = have_n ? std::min<uint64_t>(n, cap) : 0;
+    if (dev_out && !dst) return FQXV_RANS_E_INVALID_ARG;
+    CK(ctx->io_in.ensure(std::max<size_t>(len, 16), s));
+    CK(ctx->io_out.ensure(std::max<uint64_t>(dev_out, 16), s));
+    if (len) CK(cudaMemcpyAsync(ctx->io_in.p, src, len, cudaMemcpyHostToDevice, s));
+    fqxv_rans_span blk{0, len}, out{0, cap};
+    uint64_t olen = 0;
+    int32_t bst = 0;
+    st = decode_batch_impl(ctx, ctx->io_in.as<uint8_t>(), &blk, 1, UINT64_MAX, ctx->io_out.as<uint8_t>(), &out,
+                           &olen, &bst, 1);
+    if (st) return st;
+    if (olen) {
+        CK(cudaMemcpyAsync(dst, ctx->io_out.p, olen, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    *out_len = olen;
+    return FQXV_RANS_OK;
+}
+
+int fqxv_rans_decode(const uint8_t *src, size_t len, uint8_t *dst, size_t cap, size_t *out_len) {
+    return fqxv_rans_decode_bounded(src, len, SIZE_MAX, dst, cap, out_len);
+}
+
+int fqxv_rans_decode_with(const uint8_t *src, size_t len, int backend, uint8_t *dst, size_t cap,
+                          size_t *out_len) {
+    (void)backend;  // lib.rs:241-255: every backend yields the same output
+    return fqxv_rans_decode(src, len, dst, cap, out_len);
+}
+
+}  // extern "C"

@@ -1,0 +1,439 @@
+// Encode path of the B200 rANS Nx16 coder.
+//
+// Stages (each one launch over the whole batch):
+//   1. enc_model_kernel   one CTA per block: order-0 histogram (warp-private
+//      shared-memory atomics with run-length folding), exact normalisation,
+//      encode tables; for order-1 a dense |U| x |U| pair histogram and one
+//      normalised model per present context.
+//   2. enc_run_kernel     one warp per (block, order) job taken from a device
+//      work queue (jobs sorted largest first): lane l owns state l and walks
+//      the rounds from the last to the first, emitting renorm words with a
+//      ballot/popc compaction written back to front into a word scratch.
+//   3. enc_select_scan    encoded sizes, order selection, exclusive scan.
+//   4. enc_pack_kernel    one CTA per block: header, frequency tables, states
+//      and words written to their compacted place in the output arena.
+// Byte format and arithmetic follow crates/fqxv-rans/src/scalar.rs:29-140 and
+// model.rs:52-264.
+#include "rans_common.cuh"
+#include "rans_internal.cuh"
+
+namespace fqxv {
+
+namespace {
+
+__device__ __forceinline__ void unpack16(const uint4 v, uint32_t b[16]) {
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 16; k++) b[k] = (w[k >> 2] >> (8 * (k & 3))) & 0xffu;
+}
+
+// Visit p[0, n) in 16-byte aligned vector chunks (one per thread per step) and
+// in single bytes for the unaligned head and the tail. For every byte the
+// visitor gets (previous byte or 0 at position 0, byte); `flush` folds runs of
+// equal keys into one shared-memory atomic.
+template <class KeyFn, class AddFn>
+__device__ __forceinline__ void histogram_pass(const uint8_t *__restrict__ p, uint64_t n, KeyFn key,
+                                               AddFn add) {
+    const uint64_t mis = (uint64_t)(uintptr_t)p & 15u;
+    uint64_t head = mis ? 16 - mis : 0;
+    if (head > n) head = n;
+    const uint64_t body = (n - head) / 16;
+    const uint64_t tail0 = head + body * 16;
+    for (uint64_t i = threadIdx.x; i < head; i += blockDim.x) add(key(i ? p[i - 1] : 0u, p[i]), 1u);
+    for (uint64_t i = tail0 + threadIdx.x; i < n; i += blockDim.x)
+        add(key(i ? p[i - 1] : 0u, p[i]), 1u);
+    for (uint64_t c = threadIdx.x; c < body; c += blockDim.x) {
+        const uint64_t pos = head + 16 * c;
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p + pos));
+        uint32_t b[16];
+        unpack16(v, b);
+        uint32_t prev = pos ? (uint32_t)p[pos - 1] : 0u;
+        uint32_t k0 = key(prev, b[0]);
+        uint32_t run = 1;
+#pragma unroll
+        for (int k = 1; k < 16; k++) {
+            const uint32_t kk = key(b[k - 1], b[k]);
+            if (kk != k0) {
+                add(k0, run);
+                k0 = kk;
+                run = 1;
+            } else {
+                run++;
+            }
+        }
+        add(k0, run);
+    }
+}
+
+__device__ __forceinline__ uint2 enc_entry(uint32_t f, uint32_t cum) {
+    // avx2.rs:245-264: magic = floor((2^32 - 1) / f); fc = (f << 12) | cum.
+    return make_uint2(f ? 0xffffffffu / f : 0u, (f << kScaleBits) | cum);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kModelThreads)
+    enc_model_kernel(const uint8_t *__restrict__ src, EncBlock *__restrict__ blocks,
+                     const uint32_t *__restrict__ order, int nblocks, uint8_t *__restrict__ tbl,
+                     uint32_t *__restrict__ hist_scratch) {
+    constexpr int W = kModelThreads / 32;
+    constexpr int kSmemU = 64;
+    __shared__ uint32_t h0[W][256];
+    __shared__ uint32_t h1[kSmemU * kSmemU];
+    __shared__ uint32_t cnt[256];
+    __shared__ uint8_t umap[256];
+    __shared__ int s_nu, s_nctx;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint32_t *gh = hist_scratch + (size_t)blockIdx.x * 65536;
+
+    for (int bi = blockIdx.x; bi < nblocks; bi += gridDim.x) {
+        const int b = order[bi];
+        const uint8_t *p = src + blocks[b].src_off;
+        const uint64_t n = blocks[b].n;
+        const int mode = blocks[b].mode;
+        uint8_t *T = tbl + blocks[b].tbl_off;
+
+        for (int i = tid; i < W * 256; i += blockDim.x) (&h0[0][0])[i] = 0;
+        if (tid == 0) s_nctx = 0;
+        __syncthreads();
+        // Pass A: order-0 counts (scalar.rs:30-33).
+        uint32_t *hw = h0[warp];
+        histogram_pass(
+            p, n, [](uint32_t, uint32_t c) { return c; },
+            [&](uint32_t k, uint32_t r) { atomicAdd(&hw[k], r); });
+        __syncthreads();
+        if (tid < 256) {
+            uint32_t s = 0;
+#pragma unroll
+            for (int w = 0; w < W; w++) s += h0[w][tid];
+            cnt[tid] = s;
+        }
+        __syncthreads();
+
+        if (mode != FQXV_RANS_ORDER1 && warp == 0) {
+            uint32_t f[8], cum[8];
+            bool present;
+            warp_normalize(cnt, 256, f, cum, present);
+            uint2 *T0 = reinterpret_cast<uint2 *>(T + kTblO0);
+#pragma unroll
+            for (int k = 0; k < 8; k++) T0[lane * 8 + k] = enc_entry(f[k], cum[k]);
+        }
+        if (mode == FQXV_RANS_ORDER0) {
+            __syncthreads();
+            continue;
+        }
+
+        // Order-1 (scalar.rs:62-80). U = occurring bytes plus context 0, in
+        // ascending byte order; contexts and symbols share that dense index.
+        if (warp == 0) {
+            uint32_t flags = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int s = lane * 8 + k;
+                if (cnt[s] != 0 || s == 0) flags |= 1u << k;
+            }
+            const uint32_t c = __popc(flags);
+            uint32_t base = warp_incl_scan(c) - c;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int s = lane * 8 + k;
+                umap[s] = (flags >> k) & 1u ? (uint8_t)(base++) : (uint8_t)0xff;
+            }
+            if (lane == 31) s_nu = (int)(base);
+        }
+        __syncthreads();
+        const int nu = s_nu;
+        const bool in_smem = nu <= kSmemU;
+        uint32_t *H = in_smem ? h1 : gh;
+        for (int i = tid; i < nu * nu; i += blockDim.x) H[i] = 0;
+        if (tid < 256) T[kTblUmap + tid] = umap[tid];
+        __syncthreads();
+        histogram_pass(
+            p, n, [&](uint32_t prev, uint32_t c) { return (uint32_t)umap[prev] * nu + umap[c]; },
+            [&](uint32_t k, uint32_t r) { atomicAdd(&H[k], r); });
+        __syncthreads();
+        uint2 *T1 = reinterpret_cast<uint2 *>(T + kTblO1);
+        for (int t = warp; t < nu; t += W) {
+            uint32_t f[8], cum[8];
+            bool present;
+            warp_normalize(H + (size_t)t * nu, nu, f, cum, present);
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int u = lane * 8 + k;
+                if (u < nu) T1[(size_t)t * nu + u] = enc_entry(f[k], cum[k]);
+            }
+            if (lane == 0 && present) atomicAdd(&s_nctx, 1);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            blocks[b].nu = nu;
+            blocks[b].nctx = s_nctx;
+        }
+        __syncthreads();
+    }
+}
+
+// Reverse-order encode of one block by one warp (scalar.rs:39-43 / :84-90,
+// the state map of model.rs:125-133 computed as avx2.rs:383-393). Lane l owns
+// state l; round r covers positions [32r, 32r + 32). Rounds run from the last
+// to the first; the renorm words of a round are emitted high lane first, so
+// they are stored back to front at [wend - k, wend) in ascending lane order
+// and the finished region is already in decode order (scalar.rs:134-139).
+template <int ORDER>
+__device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint64_t n,
+                                            const uint2 *__restrict__ tab,
+                                            const uint8_t *__restrict__ umap, int nu,
+                                            uint16_t *__restrict__ words, uint64_t word_end,
+                                            uint64_t &nwords, uint32_t &state) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    uint32_t x = kRansL;
+    uint64_t wend = word_end;
+    const int64_t R = (int64_t)((n + 31) / 32);
+    uint32_t cur[16], nxt[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int64_t r = R - 1 - k;
+        const uint64_t i = (uint64_t)r * 32 + lane;
+        cur[k] = (r >= 0 && i < n) ? (uint32_t)__ldg(p + i) : 0u;
+    }
+    for (int64_t rtop = R - 1; rtop >= 0; rtop -= 16) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int64_t r = rtop - 16 - k;
+            const uint64_t i = (uint64_t)r * 32 + lane;
+            nxt[k] = (r >= 0 && i < n) ? (uint32_t)__ldg(p + i) : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int64_t r = rtop - k;
+            if (r < 0) break;
+            const uint64_t i = (uint64_t)r * 32 + lane;
+            const bool active = i < n;
+            const uint32_t s = cur[k];
+            uint2 e;
+            if (ORDER == 0) {
+                e = tab[s];
+            } else {
+                const uint32_t up = __shfl_up_sync(0xffffffffu, s, 1);
+                const uint32_t p31 = __shfl_sync(0xffffffffu, k < 15 ? cur[k + 1 < 16 ? k + 1 : 15] : nxt[0], 31);
+                const uint32_t prev = lane ? up : (r == 0 ? 0u : p31);
+                e = __ldg(tab + (uint32_t)umap[prev] * (uint32_t)nu + umap[s]);
+            }
+            const uint32_t f = e.y >> kScaleBits;
+            const uint32_t cum = e.y & (kTotFreq - 1);
+            // scalar.rs:122: emit while x >= x_max = f << 20 (at most once).
+            const bool need = active && (x >> 20) >= f;
+            const uint32_t mask = __ballot_sync(0xffffffffu, need);
+            const uint32_t kw = __popc(mask);
+            if (need) words[wend - kw + __popc(mask & lt)] = (uint16_t)(x & 0xffffu);
+            wend -= kw;
+            const uint32_t v = need ? x >> 16 : x;
+            uint32_t q = __umulhi(v, e.x);
+            uint32_t rem = v - q * f;
+            if (rem >= f) {
+                q += 1;
+                rem -= f;
+            }
+            if (active) x = (q << kScaleBits) + rem + cum;
+        }
+#pragma unroll
+        for (int k = 0; k < 16; k++) cur[k] = nxt[k];
+    }
+    nwords = word_end - wend;
+    state = x;
+}
+
+__global__ void __launch_bounds__(kEncWarpsPerCta * 32)
+    enc_run_kernel(const uint8_t *__restrict__ src, EncBlock *__restrict__ blocks,
+                   const EncJob *__restrict__ jobs, int njobs, const uint8_t *__restrict__ tbl,
+                   uint16_t *__restrict__ words, int *__restrict__ queue) {
+    __shared__ uint2 s_tab[kEncWarpsPerCta][256];
+    __shared__ uint8_t s_umap[kEncWarpsPerCta][256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (;;) {
+        int j = 0;
+        if (lane == 0) j = atomicAdd(queue, 1);
+        j = __shfl_sync(0xffffffffu, j, 0);
+        if (j >= njobs) return;
+        const EncJob job = jobs[j];
+        EncBlock &B = blocks[job.block];
+        const uint64_t n = B.n;
+        const uint8_t *p = src + B.src_off;
+        const uint8_t *T = tbl + B.tbl_off;
+        const uint64_t word_end = B.word_off[job.order] + n;
+        uint64_t nw = 0;
+        uint32_t st = kRansL;
+        if (n) {
+            if (job.order == 0) {
+                const uint2 *T0 = reinterpret_cast<const uint2 *>(T + kTblO0);
+#pragma unroll
+                for (int k = 0; k < 8; k++) s_tab[warp][lane * 8 + k] = T0[lane * 8 + k];
+                __syncwarp();
+                encode_warp<0>(p, n, s_tab[warp], nullptr, 0, words, word_end, nw, st);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) s_umap[warp][lane * 8 + k] = T[kTblUmap + lane * 8 + k];
+                __syncwarp();
+                encode_warp<1>(p, n, reinterpret_cast<const uint2 *>(T + kTblO1), s_umap[warp], B.nu,
+                               words, word_end, nw, st);
+            }
+        }
+        B.states[job.order][lane] = st;
+        if (lane == 0) B.nwords[job.order] = nw;
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(1024)
+    enc_select_scan_kernel(EncBlock *__restrict__ blocks, int nblocks, uint64_t *__restrict__ total) {
+    __shared__ uint64_t wtot[32];
+    __shared__ uint64_t carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nblocks; base += 1024) {
+        const int b = base + tid;
+        uint64_t size = 0;
+        if (b < nblocks) {
+            EncBlock &B = blocks[b];
+            const uint64_t n = B.n;
+            const uint64_t s0 = n ? kHdr + kO0Tables + kStatesBytes + 2 * B.nwords[0] : kHdr;
+            const uint64_t s1 =
+                n ? kHdr + kO1Bitmap + kO1Table * (uint64_t)B.nctx + kStatesBytes + 2 * B.nwords[1] : kHdr;
+            int ch;
+            switch (B.mode) {
+                case FQXV_RANS_ORDER0: ch = 0; break;
+                case FQXV_RANS_ORDER1: ch = 1; break;
+                case FQXV_RANS_BEST_TIE0: ch = s1 < s0 ? 1 : 0; break;
+                default: ch = s1 <= s0 ? 1 : 0; break;
+            }
+            B.out_size[0] = s0;
+            B.out_size[1] = s1;
+            B.chosen = ch;
+            size = ch ? s1 : s0;
+        }
+        const uint64_t incl = warp_incl_scan_u64(size);
+        if (lane == 31) wtot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint64_t v = wtot[lane];
+            const uint64_t vi = warp_incl_scan_u64(v);
+            wtot[lane] = vi - v;
+            if (lane == 31) wtot[31] = vi - v;  // keep exclusive; chunk total below
+        }
+        __syncthreads();
+        const uint64_t excl = carry + wtot[warp] + incl - size;
+        if (b < nblocks) blocks[b].out_off = excl;
+        __syncthreads();
+        if (tid == 1023) carry = excl + size;
+        __syncthreads();
+    }
+    if (tid == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kPackThreads)
+    enc_pack_kernel(const EncBlock *__restrict__ blocks, int nblocks, const uint8_t *__restrict__ tbl,
+                    const uint16_t *__restrict__ words, uint8_t *__restrict__ dst) {
+    __shared__ uint8_t present[256];
+    __shared__ uint8_t rowctx[256];
+    __shared__ int s_k;
+    const int tid = threadIdx.x;
+    for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+        const EncBlock &B = blocks[b];
+        const int o = B.chosen;
+        const uint64_t n = B.n;
+        uint8_t *d = dst + B.out_off;
+        if (tid == 0) d[0] = (uint8_t)o;
+        if (tid >= 1 && tid <= 8) d[tid] = (uint8_t)(n >> (8 * (tid - 1)));
+        if (n == 0) continue;
+        const uint8_t *T = tbl + B.tbl_off;
+        uint64_t off = kHdr;
+        if (o == 0) {
+            const uint2 *T0 = reinterpret_cast<const uint2 *>(T + kTblO0);
+            for (int s = tid; s < 256; s += blockDim.x) {
+                const uint32_t f = T0[s].y >> kScaleBits;
+                d[off + 2 * s] = (uint8_t)f;
+                d[off + 2 * s + 1] = (uint8_t)(f >> 8);
+            }
+            off += kO0Tables;
+        } else {
+            // scalar.rs:96-107: presence bitmap, then one table per present
+            // context in ascending context order.
+            const int nu = B.nu;
+            const uint8_t *um = T + kTblUmap;
+            const uint2 *T1 = reinterpret_cast<const uint2 *>(T + kTblO1);
+            if (tid < 256) {
+                const uint32_t u = um[tid];
+                bool pr = false;
+                if (u != 0xffu)
+                    for (int v = 0; v < nu && !pr; v++) pr = T1[(size_t)u * nu + v].y != 0;
+                present[tid] = pr;
+            }
+            __syncthreads();
+            if (tid < 32) {
+                uint32_t bits = 0, cntp = 0;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    bits |= (uint32_t)present[tid * 8 + k] << k;
+                    cntp += present[tid * 8 + k];
+                }
+                d[off + tid] = (uint8_t)bits;
+                uint32_t base = warp_incl_scan(cntp) - cntp;
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (present[tid * 8 + k]) rowctx[base++] = (uint8_t)(tid * 8 + k);
+                if (tid == 31) s_k = (int)base;
+            }
+            __syncthreads();
+            off += kO1Bitmap;
+            const int K = s_k;
+            for (int e = tid; e < K * 256; e += blockDim.x) {
+                const uint32_t u = um[rowctx[e >> 8]];
+                const uint32_t us = um[e & 255];
+                const uint32_t f = us != 0xffu ? (T1[(size_t)u * nu + us].y >> kScaleBits) : 0u;
+                d[off + 2 * (uint64_t)e] = (uint8_t)f;
+                d[off + 2 * (uint64_t)e + 1] = (uint8_t)(f >> 8);
+            }
+            off += kO1Table * (uint64_t)K;
+        }
+        if (tid < kStates) {
+            const uint32_t x = B.states[o][tid];
+#pragma unroll
+            for (int k = 0; k < 4; k++) d[off + 4 * tid + k] = (uint8_t)(x >> (8 * k));
+        }
+        off += kStatesBytes;
+        const uint64_t W = B.nwords[o];
+        const uint16_t *ws = words + B.word_off[o] + n - W;
+        for (uint64_t j = tid; j < W; j += blockDim.x) {
+            const uint16_t w = ws[j];
+            d[off + 2 * j] = (uint8_t)w;
+            d[off + 2 * j + 1] = (uint8_t)(w >> 8);
+        }
+        __syncthreads();
+    }
+}
+
+void launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
+                      uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s) {
+    if (nblocks <= 0) return;
+    enc_model_kernel<<<grid, kModelThreads, 0, s>>>(src, blocks, order, nblocks, tbl, hist_scratch);
+}
+
+void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,
+                    const uint8_t *tbl, uint16_t *words, int *queue, int grid, cudaStream_t s) {
+    if (njobs <= 0) return;
+    enc_run_kernel<<<grid, kEncWarpsPerCta * 32, 0, s>>>(src, blocks, jobs, njobs, tbl, words, queue);
+}
+
+void launch_enc_select_scan(EncBlock *blocks, int nblocks, uint64_t *total, cudaStream_t s) {
+    enc_select_scan_kernel<<<1, 1024, 0, s>>>(blocks, nblocks, total);
+}
+
+void launch_enc_pack(EncBlock *blocks, int nblocks, const uint8_t *tbl, const uint16_t *words,
+                     uint8_t *dst, int grid, cudaStream_t s) {
+    if (nblocks <= 0) return;
+    enc_pack_kernel<<<grid, kPackThreads, 0, s>>>(blocks, nblocks, tbl, words, dst);
+}
+
+}  // namespace fqxv

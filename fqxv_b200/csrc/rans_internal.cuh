@@ -1,0 +1,118 @@
+// Internal definitions shared by the encode, decode and C-ABI translation
+// units of libfqxv_rans_gpu.so. Nothing here is part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fqxv_rans_gpu.h"
+
+namespace fqxv {
+
+// crates/fqxv-rans/src/model.rs:9-19
+constexpr uint32_t kScaleBits = 12;
+constexpr uint32_t kTotFreq = 1u << kScaleBits;
+constexpr uint32_t kRansL = 1u << 16;
+constexpr int kStates = 32;
+
+// scalar.rs:8-20: [u8 order][u64 n] ++ tables ++ [32 x u32 states] ++ words
+constexpr uint64_t kHdr = 9;
+constexpr uint64_t kO0Tables = 512;         // 256 x u16
+constexpr uint64_t kO1Bitmap = 32;          // context presence bitmap
+constexpr uint64_t kO1Table = 512;          // 256 x u16 per present context
+constexpr uint64_t kStatesBytes = 4 * kStates;
+
+// Persistent-kernel shapes.
+constexpr int kModelThreads = 512;          // model kernel: one CTA per block
+constexpr int kEncWarpsPerCta = 4;          // encode: one warp per (block, order)
+constexpr int kDecWarpsPerCta = 4;          // decode: one warp per stream
+constexpr int kParseThreads = 256;          // decode header/table kernel
+constexpr int kPackThreads = 256;           // output compaction
+
+// Encode-side descriptor of one input block (device resident).
+struct EncBlock {
+    uint64_t src_off;       // offset of the block in the input arena
+    uint64_t n;             // block length in bytes
+    uint64_t word_off[2];   // word-scratch region (u16 units) per order; n words each
+    uint64_t tbl_off;       // table arena offset (bytes)
+    uint64_t out_off;       // compacted output offset (set by the scan)
+    uint64_t out_size[2];   // encoded size per order (set after encode)
+    uint64_t nwords[2];     // renorm words per order (set by the encoder)
+    uint32_t states[2][kStates];
+    int32_t mode;           // FQXV_RANS_ORDER0/1, BEST_TIE0/1
+    int32_t nu;             // |U|: symbols present plus context 0 (order-1 tables)
+    int32_t nctx;           // present order-1 contexts
+    int32_t chosen;         // order written to the output
+};
+
+// One encode job: a (block, order) pair; the job list is sorted by size.
+struct EncJob {
+    uint32_t block;
+    uint32_t order;
+};
+
+// Table arena layout per block (bytes from tbl_off):
+//   [0, 2048)               order-0: 256 x uint2 {magic, (freq << 12) | cum}
+//   [2048, 2048 + 256)      order-1: u8 dense index of each byte value (0xFF: not in U)
+//   [2304, ...)             order-1: nu x nu x uint2, row = context, column = symbol
+constexpr uint64_t kTblO0 = 0;
+constexpr uint64_t kTblUmap = 2048;
+constexpr uint64_t kTblO1 = 2304;
+__host__ __device__ inline uint64_t enc_table_bytes(uint64_t n) {
+    uint64_t u = n + 1 < 256 ? n + 1 : 256;
+    return kTblO1 + u * u * 8;
+}
+
+// Decode-side descriptor of one stream.
+struct DecStream {
+    uint64_t src_off, src_len;   // input span
+    uint64_t dst_off, dst_cap;   // output span
+    uint64_t max_len;            // decode_bounded bound (UINT64_MAX: none)
+    uint64_t n;                  // declared output length
+    uint64_t words_off;          // absolute byte offset of the renorm words
+    uint64_t words_len;          // bytes after the header
+    uint64_t tbl_off;            // table arena offset (bytes)
+    int32_t order;
+    int32_t status;
+    int32_t nctx;
+    int32_t ctx0;                // dense index of context 0 (0xFF: absent)
+    uint32_t states[kStates];
+};
+
+// Decode table arena per stream (bytes from tbl_off):
+//   order-0: 4096 x u32 packed ((freq - 1) << 20) | ((slot - cum) << 8) | sym
+//   order-1: [256 B] raw context -> dense index (0xFF absent), then per dense
+//            context t: 4096 x u16 (sym << 8) | dense(sym), then 256 x u32
+//            (freq << 12) | cum.
+constexpr uint64_t kDecCtxMap = 0;
+constexpr uint64_t kDecO1Base = 256;
+constexpr uint64_t kDecO1Slot = 4096 * 2;
+constexpr uint64_t kDecO1Fc = 256 * 4;
+constexpr uint64_t kDecO1Ctx = kDecO1Slot + kDecO1Fc;
+__host__ __device__ inline uint64_t dec_table_bytes(uint64_t src_len) {
+    // A stream with K order-1 tables is at least 41 + 512 K bytes long.
+    uint64_t k = src_len > 41 ? (src_len - 41) / 512 : 0;
+    if (k > 256) k = 256;
+    uint64_t o1 = kDecO1Base + k * kDecO1Ctx;
+    return o1 > 16384 ? o1 : 16384;
+}
+
+inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+// ---- launchers (rans_encode.cu / rans_decode.cu) ---------------------------
+void launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
+                      uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s);
+void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,
+                    const uint8_t *tbl, uint16_t *words, int *queue, int grid, cudaStream_t s);
+void launch_enc_select_scan(EncBlock *blocks, int nblocks, uint64_t *total, cudaStream_t s);
+void launch_enc_pack(EncBlock *blocks, int nblocks, const uint8_t *tbl, const uint16_t *words,
+                     uint8_t *dst, int grid, cudaStream_t s);
+
+void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint8_t *tbl,
+                      int grid, cudaStream_t s);
+void launch_dec_run(const uint8_t *src, DecStream *streams, const uint32_t *order, int nstreams,
+                    const uint8_t *tbl, uint8_t *dst, int *queue, int grid, cudaStream_t s);
+
+int sm_count(int device);
+
+}  // namespace fqxv

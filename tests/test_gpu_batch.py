@@ -1,0 +1,142 @@
+"""Batched device API parity: many blocks per pass, against the oracle block
+by block; batched and plain per-block forms give the same bytes; full-size
+workloads checked through round trips and against the oracle."""
+
+import numpy as np
+import pytest
+
+from fqxv_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def codec():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from fqxv_b200.batch import Codec
+
+    c = Codec(0)
+    yield c
+    c.close()
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+
+def _oracle_best(orc, blk, tie_to_one=False):
+    e0, e1 = orc.encode(blk, 0), orc.encode(blk, 1)
+    if tie_to_one:
+        return e1 if len(e1) <= len(e0) else e0
+    return e1 if len(e1) < len(e0) else e0
+
+
+def _roundtrip_check(codec, data, spans, d_out, out_spans):
+    import torch
+
+    dsp = out_spans.copy()
+    dst = np.zeros_like(spans)
+    dst[:, 0] = spans[:, 0]
+    dst[:, 1] = spans[:, 1]
+    d_dec, lens, st = codec.decode_batch(d_out, dsp, dst)
+    assert (st == 0).all()
+    assert (lens == spans[:, 1]).all()
+    torch.cuda.synchronize()
+    assert np.array_equal(d_dec[:len(data)].cpu().numpy(), data)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_mixed_batch_matches_oracle(codec, orc, mode):
+    data, spans, kinds = W.config2(nblocks=48, lo=1, hi=300_000, seed=100 + mode)
+    d_src = _dev(data)
+    d_out, out_spans, orders = codec.encode_batch(d_src, spans, mode)
+    out = d_out.cpu().numpy()
+    pos = 0
+    for i, (off, ln) in enumerate(spans):
+        blk = data[int(off):int(off + ln)].tobytes()
+        if mode in (0, 1):
+            ref = orc.encode(blk, mode)
+        else:
+            ref = _oracle_best(orc, blk, tie_to_one=(mode == 3))
+        o, l = int(out_spans[i, 0]), int(out_spans[i, 1])
+        assert o == pos, "streams are back to back in block order"
+        assert out[o:o + l].tobytes() == ref, (i, kinds[i], len(blk))
+        assert orders[i] == ref[0]
+        pos += l
+    _roundtrip_check(codec, data, spans, d_out, out_spans)
+
+
+def test_plain_form_equals_batched(codec):
+    data, spans, _ = W.config2(nblocks=24, lo=100, hi=200_000, seed=7)
+    d_src = _dev(data)
+    for mode in (0, 1, 2):
+        a, sa, oa = codec.encode_batch(d_src, spans, mode, persistent=True)
+        b, sb, ob = codec.encode_batch(d_src, spans, mode, persistent=False)
+        assert np.array_equal(sa, sb) and np.array_equal(oa, ob)
+        n = int(sa[-1, 0] + sa[-1, 1])
+        assert np.array_equal(a[:n].cpu().numpy(), b[:n].cpu().numpy())
+        dst = spans.copy()
+        d1, l1, s1 = codec.decode_batch(a, sa, dst, persistent=True)
+        d2, l2, s2 = codec.decode_batch(a, sa, dst, persistent=False)
+        assert (s1 == 0).all() and (s2 == 0).all()
+        assert np.array_equal(d1[:len(data)].cpu().numpy(), d2[:len(data)].cpu().numpy())
+
+
+def test_config0_binned_order0_full_size(codec, orc):
+    data, spans = W.config0()
+    d_out, sp, _ = codec.encode_batch(_dev(data), spans, 0)
+    ref = orc.encode(data.tobytes(), 0)
+    assert d_out[:int(sp[0, 1])].cpu().numpy().tobytes() == ref
+    _roundtrip_check(codec, data, spans, d_out, sp)
+
+
+def test_config1_full_quality_order1_full_size(codec, orc):
+    data, spans = W.config1()
+    d_out, sp, _ = codec.encode_batch(_dev(data), spans, 1)
+    out = d_out.cpu().numpy()
+    ref, roff, rlen = orc.encode_batch(data, spans[:, 0], spans[:, 1], 1)
+    for i in range(len(spans)):
+        got = out[int(sp[i, 0]):int(sp[i, 0] + sp[i, 1])]
+        want = ref[int(roff[i]):int(roff[i] + rlen[i])]
+        assert np.array_equal(got, want), i
+    _roundtrip_check(codec, data, spans, d_out, sp)
+
+
+def test_ont_blocks_cpu_encoded_gpu_decoded(codec, orc):
+    data, spans = W.config3_ont(nreads=120, lo=64 << 10, hi=1 << 20, seed=3)
+    enc, eoff, elen = orc.encode_batch(data, spans[:, 0], spans[:, 1], 1)
+    cs = np.stack([eoff, elen], axis=1)
+    d_dec, lens, st = codec.decode_batch(_dev(enc), cs, spans)
+    assert (st == 0).all() and (lens == spans[:, 1]).all()
+    assert np.array_equal(d_dec[:len(data)].cpu().numpy(), data)
+
+
+def test_decode_batch_per_block_status(codec, orc):
+    rng = np.random.default_rng(1)
+    streams, want = [], []
+    for i in range(40):
+        blk = rng.integers(0, 30, int(rng.integers(0, 5000))).astype(np.uint8).tobytes()
+        e = bytearray(orc.encode(blk, i % 2))
+        if i % 3 == 0 and len(e) > 20:
+            e = e[:int(rng.integers(9, len(e)))]
+        if i % 5 == 0 and len(e) > 12:
+            e[10] ^= 0x5A
+        streams.append(bytes(e))
+        want.append(orc.decode_status(bytes(e), max_len=1 << 16))
+    lens = np.array([len(s) for s in streams], np.uint64)
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint64)
+    arena = np.frombuffer(b"".join(streams), np.uint8)
+    caps = np.full(40, 1 << 16, np.uint64)
+    doffs = (np.arange(40, dtype=np.uint64) << np.uint64(16))
+    d_dec, olens, st = codec.decode_batch(_dev(arena), np.stack([offs, lens], 1), np.stack([doffs, caps], 1),
+                                          max_len=1 << 16, raise_on_error=False)
+    dec = d_dec.cpu().numpy()
+    for i, (ws, wb) in enumerate(want):
+        assert st[i] == ws, i
+        if ws == 0:
+            assert dec[int(doffs[i]):int(doffs[i]) + int(olens[i])].tobytes() == wb
