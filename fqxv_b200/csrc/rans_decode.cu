@@ -147,9 +147,11 @@ __global__ void __launch_bounds__(kParseThreads)
         }
         if (status == FQXV_RANS_OK && tid < kStates) S.states[tid] = ld_u32_le(p + hdr + 4 * tid);
         if (tid == 0) {
+            // The renorm words follow the 32 states (scalar.rs:130-140).
+            const uint64_t wbeg = hdr + kStatesBytes;
             S.status = status;
-            S.words_off = S.src_off + hdr;
-            S.words_len = L > hdr ? L - hdr : 0;
+            S.words_off = S.src_off + wbeg;
+            S.words_len = L > wbeg ? L - wbeg : 0;
         }
         __syncthreads();
     }

@@ -67,7 +67,10 @@ __device__ __forceinline__ void histogram_pass(const uint8_t *__restrict__ p, ui
 
 __device__ __forceinline__ uint2 enc_entry(uint32_t f, uint32_t cum) {
     // avx2.rs:245-264: magic = floor((2^32 - 1) / f); fc = (f << 12) | cum.
-    return make_uint2(f ? 0xffffffffu / f : 0u, (f << kScaleBits) | cum);
+    // Absent symbols get an all-zero entry (their cum can be 4096, which
+    // would otherwise spill into the frequency field).
+    if (f == 0) return make_uint2(0u, 0u);
+    return make_uint2(0xffffffffu / f, (f << kScaleBits) | cum);
 }
 
 }  // namespace
@@ -363,10 +366,13 @@ __global__ void __launch_bounds__(kPackThreads)
             const int nu = B.nu;
             const uint8_t *um = T + kTblUmap;
             const uint2 *T1 = reinterpret_cast<const uint2 *>(T + kTblO1);
+            // With all 256 byte values in U the map is the identity and 0xFF
+            // is a real index, not the "absent" marker.
+            const bool full = nu == 256;
             if (tid < 256) {
                 const uint32_t u = um[tid];
                 bool pr = false;
-                if (u != 0xffu)
+                if (full || u != 0xffu)
                     for (int v = 0; v < nu && !pr; v++) pr = T1[(size_t)u * nu + v].y != 0;
                 present[tid] = pr;
             }
@@ -391,7 +397,7 @@ __global__ void __launch_bounds__(kPackThreads)
             for (int e = tid; e < K * 256; e += blockDim.x) {
                 const uint32_t u = um[rowctx[e >> 8]];
                 const uint32_t us = um[e & 255];
-                const uint32_t f = us != 0xffu ? (T1[(size_t)u * nu + us].y >> kScaleBits) : 0u;
+                const uint32_t f = (full || us != 0xffu) ? (T1[(size_t)u * nu + us].y >> kScaleBits) : 0u;
                 d[off + 2 * (uint64_t)e] = (uint8_t)f;
                 d[off + 2 * (uint64_t)e + 1] = (uint8_t)(f >> 8);
             }

@@ -26,7 +26,7 @@ def codec():
 def _dev(a):
     import torch
 
-    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+    return torch.from_numpy(np.array(a, dtype=np.uint8, copy=True)).to("cuda")
 
 
 def _oracle_best(orc, blk, tie_to_one=False):
