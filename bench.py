@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 rANS Nx16 coder.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config1]
+    python bench.py --impl reference ...      # the CPU arm
+
+A step is one pass of the hot path over one batch: batched encode of every
+block of the workload, then batched decode of the streams just written.
+`value` is uncompressed GB/s (decimal) of that round trip with the input
+resident in HBM, summed over ranks (weak scaling: every rank codes its own
+seeded copy of the workload; blocks are independent, there is no collective
+on the data path). L2 is flushed (a 256 MiB write) before every timed step.
+
+Workloads (seeded synthetic data of the benchmark shapes):
+  config1  64 x 1 MiB full-range quality, order-1                 (default)
+  config0  1 x 1 MiB binned quality, order-0
+  config2  4096 mixed blocks 4 KiB - 4 MiB, both orders, keep the smaller
+  config3  config2 (CPU-encoded) + ONT long-read blocks, decode only
+
+The reference arm (`--impl reference`) times the reference's CPU coder -- the
+C restatement of fqxv-rans (AVX-512/AVX2 order-0, scalar order-1) -- with all
+host threads over the same workload, on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from fqxv_b200 import workloads as W  # noqa: E402
+
+METRIC = "rANS Nx16 enc/dec GB/s, bit-exact (uncompressed bytes per second, encode + decode round trip)"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def build_workload(name: str, seed: int):
+    """-> (data u8, spans (n,2), encode order or None for decode-only, description, extra)."""
+    if name == "config1":
+        data, spans = W.config1(seed=seed)
+        return data, spans, 1, "64 x 1 MiB full-range quality blocks, order-1", {}
+    if name == "config0":
+        data, spans = W.config0(seed=seed)
+        return data, spans, 0, "1 x 1 MiB binned quality block, order-0", {}
+    if name == "config2":
+        data, spans, kinds = W.config2(seed=seed)
+        return data, spans, 2, "4096 mixed blocks 4 KiB-4 MiB, both orders, keep the smaller", {}
+    if name == "config3":
+        d2, s2, _ = W.config2(seed=seed)
+        d3, s3 = W.config3_ont(seed=seed)
+        s3 = s3.copy()
+        s3[:, 0] += len(d2)
+        data = np.concatenate([d2, d3])
+        spans = np.concatenate([s2, s3])
+        return data, spans, None, "config2 blocks (CPU-encoded, best order) + ONT quality blocks (order-1), decode", \
+            {"n_ont_blocks": int(len(s3))}
+    raise SystemExit("unknown workload %s" % name)
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def oracle_roundtrip(data, spans, order, nthreads=0):
+    """One CPU pass: encode every block then decode it (the reference's
+    rayon-over-blocks shape on all host threads). Returns (enc arena, offs, lens)."""
+    from oracle import oracle
+
+    enc, eoff, elen = oracle.encode_batch(data, spans[:, 0], spans[:, 1], order, nthreads)
+    dec, _, dlen = oracle.decode_batch(enc, eoff, elen, spans[:, 1], nthreads)
+    return enc, eoff, elen
+
+
+def cpu_encoded(data, spans, seed_tag):
+    """CPU-encoded streams for the decode-only workload (reference encoder,
+    best order with the tokenizer's tie rule)."""
+    from oracle import oracle
+
+    enc, eoff, elen = oracle.encode_batch(data, spans[:, 0], spans[:, 1], 2)
+    # compact
+    parts = [enc[int(o):int(o + l)] for o, l in zip(eoff, elen)]
+    arena = np.concatenate(parts) if parts else np.zeros(0, np.uint8)
+    offs = np.zeros(len(parts), np.uint64)
+    if len(parts):
+        offs[1:] = np.cumsum(elen)[:-1]
+    return arena, np.stack([offs, elen.astype(np.uint64)], 1)
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    data, spans, order, desc, extra = build_workload(args.workload, args.seed)
+    nthreads = os.cpu_count() or 1
+    n_bytes = int(spans[:, 1].sum())
+    from oracle import oracle
+
+    if order is None:
+        arena, cspans = cpu_encoded(data, spans, args.seed)
+
+        def step():
+            oracle.decode_batch(arena, cspans[:, 0], cspans[:, 1], spans[:, 1], nthreads)
+    else:
+        def step():
+            oracle_roundtrip(data, spans, order, nthreads)
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    gbs = n_bytes * args.steps / dt / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": dict({"workload": args.workload, "desc": desc, "blocks": int(len(spans)), "bytes": n_bytes}, **extra),
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": nthreads, "kind": "port",
+                         "sample": "the whole workload every step (C restatement of fqxv-rans: AVX-512/AVX2 "
+                                   "order-0, scalar order-1), all host threads over blocks"},
+        "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="config1", choices=["config1", "config0", "config2", "config3"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+
+    from fqxv_b200.batch import Codec
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    data, spans, order, desc, extra = build_workload(args.workload, args.seed + rank)
+    n_bytes = int(spans[:, 1].sum())
+    codec = Codec(local)
+    cs = torch.cuda.ExternalStream(codec.stream_handle)
+    d_src = torch.from_numpy(data).to("cuda")
+    d_dec = torch.empty(max(n_bytes, 1), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    decode_only = order is None
+    if decode_only:
+        arena, cspans = cpu_encoded(data, spans, args.seed)
+        d_enc = torch.from_numpy(arena).to("cuda")
+        enc_spans = cspans
+        comp_bytes = int(cspans[:, 1].sum())
+    else:
+        d_enc = torch.empty(max(codec.encode_bound(spans, order), 1), dtype=torch.uint8, device="cuda")
+        enc_spans = None
+        comp_bytes = 0
+
+    def step(persistent=True):
+        nonlocal enc_spans, comp_bytes
+        if not decode_only:
+            _, enc_spans, _ = codec.encode_batch(d_src, spans, order, d_dst=d_enc, persistent=persistent)
+            comp_bytes = int(enc_spans[:, 1].sum())
+        _, lens, st = codec.decode_batch(d_enc, enc_spans, spans, d_dst=d_dec, persistent=persistent)
+        return st
+
+    for _ in range(args.warmup):
+        st = step()
+    torch.cuda.synchronize()
+    assert (st == 0).all() and torch.equal(d_dec[:n_bytes], d_src[:n_bytes]), "round trip mismatch"
+
+    # ---- timed region ---------------------------------------------------
+    codec.stage_stats(reset=True)
+    codec.set_profiling(True)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    total_ms = 0.0
+    enc_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(cs)
+        if not decode_only:
+            _, enc_spans, _ = codec.encode_batch(d_src, spans, order, d_dst=d_enc)
+        e1.record(cs)
+        codec.decode_batch(d_enc, enc_spans, spans, d_dst=d_dec)
+        e2.record(cs)
+        e2.synchronize()
+        total_ms += e0.elapsed_time(e2)
+        enc_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    codec.set_profiling(False)
+    stages = codec.stage_stats(reset=True)
+    if not decode_only:
+        comp_bytes = int(enc_spans[:, 1].sum())
+
+    t = torch.tensor([total_ms, enc_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, enc_ms = float(t[0]), float(t[1])
+    dec_ms = total_ms - enc_ms
+    value = world * n_bytes * args.steps / (total_ms * 1e-3) / 1e9
+
+    # ---- the dominant kernel against the HBM roofline -------------------------
+    pk = peaks()
+    timed = {k: v for k, v in stages.items() if v["launches"] > 0}
+    dom = max(timed, key=lambda k: timed[k]["ms"])
+    per_launch_ms = timed[dom]["ms"] / timed[dom]["launches"]
+    # Algorithmic bytes of one launch: the coder reads its input once and
+    # writes its output once -- n + compressed for the run/model kernels of a
+    # batch (tables are on chip and excluded).
+    alg_bytes = n_bytes + comp_bytes
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tr = json.load(f)
+        ent = tr.get(args.workload, {}).get(dom)
+        if ent:
+            traffic = ent.get("dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 5), "traffic": traffic,
+                "alg_bytes_per_launch": alg_bytes, "launch_ms": round(per_launch_ms, 4),
+                "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"}
+    gpu_launches = int(sum(v["launches"] for v in stages.values()))
+
+    # ---- plain one-block-per-launch form (same bytes) -------------------------
+    plain = None
+    if not args.no_plain and rank == 0:
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cs)
+        st = step(persistent=False)
+        b.record(cs)
+        b.synchronize()
+        ok = bool((st == 0).all()) and torch.equal(d_dec[:n_bytes], d_src[:n_bytes])
+        plain = {"gbs": round(n_bytes / (a.elapsed_time(b) * 1e-3) / 1e9, 4), "round_trip_ok": ok}
+
+    # ---- end to end through the C ABI with pinned host buffers ---------------
+    h_src = torch.from_numpy(data).pin_memory().numpy()
+    h_dec = torch.empty(max(n_bytes, 1), dtype=torch.uint8).pin_memory().numpy()
+    if decode_only:
+        h_enc = torch.from_numpy(arena).pin_memory().numpy()
+    else:
+        h_enc = torch.empty(max(codec.encode_bound(spans, order), 1), dtype=torch.uint8).pin_memory().numpy()
+
+    def e2e_step():
+        if decode_only:
+            es = enc_spans
+        else:
+            es, _ = codec.encode_batch_host(h_src, spans, order, h_enc)
+        codec.decode_batch_host(h_enc, es, spans, h_dec)
+        return es
+
+    es = e2e_step()
+    assert np.array_equal(h_dec[:n_bytes], data[:n_bytes]), "e2e round trip mismatch"
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cs)
+        es = e2e_step()
+        b.record(cs)
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t[0])
+    cb = int(es[:, 1].sum())
+    e2e = {"value": round(world * n_bytes * args.steps / (e2e_ms * 1e-3) / 1e9, 4), "unit": "GB/s",
+           "h2d_bytes_per_step": (0 if decode_only else n_bytes) + cb,
+           "d2h_bytes_per_step": (0 if decode_only else cb) + n_bytes,
+           "path": "fqxv_rans_encode_batch_host + fqxv_rans_decode_batch_host (pinned host buffers)"}
+
+    # ---- CPU baseline (rank 0, N = 1) -----------------------------------------
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        from oracle import oracle
+
+        nthreads = os.cpu_count() or 1
+        if decode_only:
+            def cstep():
+                oracle.decode_batch(arena, enc_spans[:, 0], enc_spans[:, 1], spans[:, 1], nthreads)
+        else:
+            def cstep():
+                oracle_roundtrip(data, spans, order, nthreads)
+        cstep()
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            cstep()
+            reps += 1
+            if time.perf_counter() - t0 > 5.0 or reps >= 20:
+                break
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(n_bytes * reps / dt / 1e9, 4), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": "%d passes of the whole workload (C restatement of fqxv-rans CPU path: AVX-512/AVX2 "
+                         "order-0, scalar order-1), block-parallel over %d host threads" % (reps, nthreads)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": dict({"workload": args.workload, "desc": desc, "blocks": int(len(spans)),
+                            "bytes_per_gpu": n_bytes, "compressed_bytes_per_gpu": comp_bytes,
+                            "l2": "flushed (256 MiB write) before every timed step",
+                            "parallelism": "replicas" if world > 1 else "single GPU"}, **extra),
+            "encode_gbs": None if decode_only else round(world * n_bytes * args.steps / (enc_ms * 1e-3) / 1e9, 4),
+            "decode_gbs": round(world * n_bytes * args.steps / (dec_ms * 1e-3) / 1e9, 4),
+            "plain_per_block": plain,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": gpu_launches,
+            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4)} for k, v in stages.items()},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    codec.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

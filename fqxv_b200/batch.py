@@ -15,6 +15,10 @@ import numpy as np
 from . import rans
 
 
+class StageStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double)]
+
+
 def _spans(a) -> np.ndarray:
     a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64).reshape(-1, 2))
     return a
@@ -91,3 +95,44 @@ class Codec:
         if st and (raise_on_error or st not in rans.MALFORMED):
             rans.raise_for(st)
         return d_dst, lens, status
+
+    # ---- host-buffer batch forms ------------------------------------------
+
+    def encode_batch_host(self, h_src: np.ndarray, spans, order: int, h_dst: np.ndarray):
+        """Encode blocks of a host arena (pinned for DMA speed) into h_dst."""
+        s = _spans(spans)
+        nb = len(s)
+        out = np.zeros((nb, 2), dtype=np.uint64)
+        orders = np.zeros(nb, dtype=np.int32)
+        st = self._lib.fqxv_rans_encode_batch_host(self._h, h_src.ctypes.data, s.ctypes.data, nb, int(order),
+                                                   h_dst.ctypes.data, h_dst.size, out.ctypes.data,
+                                                   orders.ctypes.data)
+        rans.raise_for(st)
+        return out, orders
+
+    def decode_batch_host(self, h_src: np.ndarray, spans, out_spans, h_dst: np.ndarray,
+                          max_len: int | None = None):
+        s = _spans(spans)
+        o = _spans(out_spans)
+        nb = len(s)
+        lens = np.zeros(nb, dtype=np.uint64)
+        status = np.zeros(nb, dtype=np.int32)
+        ml = (1 << 64) - 1 if max_len is None else int(max_len)
+        st = self._lib.fqxv_rans_decode_batch_host(self._h, h_src.ctypes.data, s.ctypes.data, nb, ml,
+                                                   h_dst.ctypes.data, o.ctypes.data, lens.ctypes.data,
+                                                   status.ctypes.data)
+        rans.raise_for(st)
+        return lens, status
+
+    # ---- per-stage timing ---------------------------------------------------
+
+    def set_profiling(self, on: bool) -> None:
+        rans.raise_for(self._lib.fqxv_rans_ctx_set_profiling(self._h, 1 if on else 0))
+
+    def stage_stats(self, reset: bool = False) -> dict:
+        arr = (StageStat * 16)()
+        n = ctypes.c_int(0)
+        rans.raise_for(self._lib.fqxv_rans_ctx_stage_stats(self._h, ctypes.cast(arr, ctypes.c_void_p), 16,
+                                                           ctypes.byref(n), 1 if reset else 0))
+        return {arr[i].name.decode(): {"launches": int(arr[i].launches), "ms": float(arr[i].ms)}
+                for i in range(n.value)}

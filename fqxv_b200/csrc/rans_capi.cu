@@ -74,6 +74,71 @@ struct HostBuf {
     }
 };
 
+enum Stage { kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecRun, kStages };
+const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan",
+                                          "enc_pack", "dec_parse", "dec_run"};
+
+// CUDA-event brackets around each kernel launch on the context's stream.
+// Durations are collected after the call's final synchronisation.
+struct StageTimer {
+    bool on = false;
+    struct Pending {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    double ms[kStages] = {};
+    uint64_t launches[kStages] = {};
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return e;
+    }
+    // Returns the start event (or null); pass it to end().
+    cudaEvent_t begin(cudaStream_t s) {
+        if (!on) return nullptr;
+        cudaEvent_t a = get();
+        if (a) cudaEventRecord(a, s);
+        return a;
+    }
+    void end(int stage, cudaEvent_t a, cudaStream_t s) {
+        launches[stage]++;
+        if (!a) return;
+        cudaEvent_t b = get();
+        if (!b) return;
+        cudaEventRecord(b, s);
+        pending.push_back({stage, a, b});
+    }
+    void collect() {
+        for (auto &p : pending) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.stage] += t;
+            else cudaGetLastError();
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void release() {
+        for (auto &p : pending) {
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+        for (auto e : pool) cudaEventDestroy(e);
+        pool.clear();
+    }
+};
+
 }  // namespace
 
 struct fqxv_rans_ctx {
@@ -88,6 +153,8 @@ struct fqxv_rans_ctx {
     // single-call staging
     DevBuf io_in, io_out;
     HostBuf h_stage;
+    HostBuf h_io;
+    StageTimer timer;
     uint64_t device_bytes() const {
         const DevBuf *all[] = {&e_blocks, &e_order, &e_jobs, &e_tbl, &e_words, &e_hist, &e_misc,
                                &d_streams, &d_order, &d_tbl, &d_misc, &io_in, &io_out};
@@ -202,18 +269,31 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     uint32_t *dH = ctx->e_hist.as<uint32_t>();
     const int run_grid = ctx->sms * 16;
     if (persistent) {
+        cudaEvent_t t0 = ctx->timer.begin(s);
         launch_enc_model(d_src, dB, dO, (int)nb, dT, dH, model_grid, s);
-        launch_enc_run(d_src, dB, dJ, (int)jobs.size(), dT, dW, queue, std::min<int>(run_grid, (int)(jobs.size() + 3) / 4), s);
+        ctx->timer.end(kStEncModel, t0, s);
+        t0 = ctx->timer.begin(s);
+        launch_enc_run(d_src, dB, dJ, (int)jobs.size(), dT, dW, queue,
+                       std::min<int>(run_grid, (int)(jobs.size() + 3) / 4), s);
+        ctx->timer.end(kStEncRun, t0, s);
     } else {
         // The plain form: every block gets its own launches, one after the other.
         const int per = (o0 && o1) ? 2 : 1;
         for (size_t j = 0; j < nb; j++) {
             CK(cudaMemsetAsync(queue, 0, 4, s));
+            cudaEvent_t t0 = ctx->timer.begin(s);
             launch_enc_model(d_src, dB, dO + j, 1, dT, dH, 1, s);
+            ctx->timer.end(kStEncModel, t0, s);
+            t0 = ctx->timer.begin(s);
             launch_enc_run(d_src, dB, dJ + j * per, per, dT, dW, queue, 1, s);
+            ctx->timer.end(kStEncRun, t0, s);
         }
     }
-    launch_enc_select_scan(dB, (int)nb, total, s);
+    {
+        cudaEvent_t t0 = ctx->timer.begin(s);
+        launch_enc_select_scan(dB, (int)nb, total, s);
+        ctx->timer.end(kStEncScan, t0, s);
+    }
     CK(cudaGetLastError());
     if (bound > dst_cap) {
         uint64_t tot = 0;
@@ -222,13 +302,20 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         if (tot > dst_cap) return FQXV_RANS_E_DST_TOO_SMALL;
     }
     if (persistent) {
+        cudaEvent_t t0 = ctx->timer.begin(s);
         launch_enc_pack(dB, (int)nb, dT, dW, d_dst, (int)std::min<size_t>(nb, (size_t)ctx->sms * 8), s);
+        ctx->timer.end(kStEncPack, t0, s);
     } else {
-        for (size_t j = 0; j < nb; j++) launch_enc_pack(dB + j, 1, dT, dW, d_dst, 1, s);
+        for (size_t j = 0; j < nb; j++) {
+            cudaEvent_t t0 = ctx->timer.begin(s);
+            launch_enc_pack(dB + j, 1, dT, dW, d_dst, 1, s);
+            ctx->timer.end(kStEncPack, t0, s);
+        }
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(hs, dB, szb, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    ctx->timer.collect();
     const EncBlock *rb = reinterpret_cast<const EncBlock *>(hs);
     for (size_t i = 0; i < nb; i++) {
         out_spans[i].offset = rb[i].out_off;
@@ -279,19 +366,28 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     const uint32_t *dO = ctx->d_order.as<uint32_t>();
     uint8_t *dT = ctx->d_tbl.as<uint8_t>();
     if (persistent) {
+        cudaEvent_t t0 = ctx->timer.begin(s);
         launch_dec_parse(d_src, dS, (int)nb, dT, (int)std::min<size_t>(nb, (size_t)ctx->sms * 8), s);
+        ctx->timer.end(kStDecParse, t0, s);
+        t0 = ctx->timer.begin(s);
         launch_dec_run(d_src, dS, dO, (int)nb, dT, d_dst, queue,
                        (int)std::min<size_t>((nb + 3) / 4, (size_t)ctx->sms * 16), s);
+        ctx->timer.end(kStDecRun, t0, s);
     } else {
         for (size_t j = 0; j < nb; j++) {
             CK(cudaMemsetAsync(queue, 0, 4, s));
+            cudaEvent_t t0 = ctx->timer.begin(s);
             launch_dec_parse(d_src, dS + ord[j], 1, dT, 1, s);
+            ctx->timer.end(kStDecParse, t0, s);
+            t0 = ctx->timer.begin(s);
             launch_dec_run(d_src, dS, dO + j, 1, dT, d_dst, queue, 1, s);
+            ctx->timer.end(kStDecRun, t0, s);
         }
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(hst, dS, szs, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    ctx->timer.collect();
     const DecStream *rs = reinterpret_cast<const DecStream *>(hst);
     int first = FQXV_RANS_OK;
     for (size_t i = 0; i < nb; i++) {
@@ -385,6 +481,8 @@ void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
                      &ctx->d_misc, &ctx->io_in, &ctx->io_out};
     for (auto *b : all) b->release();
     ctx->h_stage.release();
+    ctx->h_io.release();
+    ctx->timer.release();
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -496,6 +594,99 @@ int fqxv_rans_decode_with(const uint8_t *src, size_t len, int backend, uint8_t *
                           size_t *out_len) {
     (void)backend;  // lib.rs:241-255: every backend yields the same output
     return fqxv_rans_decode(src, len, dst, cap, out_len);
+}
+
+int fqxv_rans_ctx_set_profiling(fqxv_rans_ctx *ctx, int on) {
+    if (!ctx) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->timer.on = on != 0;
+    return FQXV_RANS_OK;
+}
+
+int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int cap, int *n, int reset) {
+    if (!ctx || !n || (cap > 0 && !out)) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    int k = 0;
+    for (int i = 0; i < kStages && k < cap; i++, k++) {
+        std::memset(out[k].name, 0, sizeof out[k].name);
+        std::strncpy(out[k].name, kStageNames[i], sizeof out[k].name - 1);
+        out[k].launches = ctx->timer.launches[i];
+        out[k].ms = ctx->timer.ms[i];
+    }
+    *n = k;
+    if (reset) {
+        for (int i = 0; i < kStages; i++) {
+            ctx->timer.launches[i] = 0;
+            ctx->timer.ms[i] = 0.0;
+        }
+    }
+    return FQXV_RANS_OK;
+}
+
+int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
+                                size_t nblocks, int order, uint8_t *h_dst, uint64_t dst_cap,
+                                fqxv_rans_span *out_spans, int32_t *out_orders) {
+    if (!ctx || (nblocks && (!blocks || !out_spans || !h_dst || !h_src))) return FQXV_RANS_E_INVALID_ARG;
+    if (nblocks == 0) return FQXV_RANS_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = ctx->stream;
+    uint64_t end = 0;
+    for (size_t i = 0; i < nblocks; i++) end = std::max<uint64_t>(end, blocks[i].offset + blocks[i].length);
+    const uint64_t bound = fqxv_rans_encode_batch_bound(blocks, nblocks, order);
+    CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
+    CK(ctx->io_out.ensure(std::max<uint64_t>(bound, 16), s));
+    CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
+    int st = encode_batch_impl(ctx, ctx->io_in.as<uint8_t>(), blocks, nblocks, order, ctx->io_out.as<uint8_t>(),
+                               bound, out_spans, out_orders, 1);
+    if (st) return st;
+    const uint64_t total = out_spans[nblocks - 1].offset + out_spans[nblocks - 1].length;
+    if (total > dst_cap) return FQXV_RANS_E_DST_TOO_SMALL;
+    CK(cudaMemcpyAsync(h_dst, ctx->io_out.p, total, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return FQXV_RANS_OK;
+}
+
+int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
+                                size_t nblocks, uint64_t max_len, uint8_t *h_dst,
+                                const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status) {
+    if (!ctx || (nblocks && (!blocks || !out_spans || !h_src || !h_dst))) return FQXV_RANS_E_INVALID_ARG;
+    if (nblocks == 0) return FQXV_RANS_OK;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = ctx->stream;
+    uint64_t end = 0, oend = 0;
+    for (size_t i = 0; i < nblocks; i++) {
+        end = std::max<uint64_t>(end, blocks[i].offset + blocks[i].length);
+        oend = std::max<uint64_t>(oend, out_spans[i].offset + out_spans[i].length);
+    }
+    CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
+    CK(ctx->io_out.ensure(std::max<uint64_t>(oend, 16), s));
+    CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
+    std::vector<uint64_t> lens(nblocks);
+    std::vector<int32_t> sts(nblocks);
+    const int first = decode_batch_impl(ctx, ctx->io_in.as<uint8_t>(), blocks, nblocks, max_len,
+                                        ctx->io_out.as<uint8_t>(), out_spans, lens.data(), sts.data(), 1);
+    if (first != FQXV_RANS_OK && (first < FQXV_RANS_E_TRUNCATED || first > FQXV_RANS_E_TRUNCATED_RENORM))
+        return first;
+    // One copy of the whole output range when the spans are dense, else one
+    // copy per decoded block.
+    uint64_t produced = 0;
+    for (size_t i = 0; i < nblocks; i++) produced += lens[i];
+    if (produced == oend && first == FQXV_RANS_OK) {
+        CK(cudaMemcpyAsync(h_dst, ctx->io_out.p, oend, cudaMemcpyDeviceToHost, s));
+    } else {
+        for (size_t i = 0; i < nblocks; i++)
+            if (lens[i])
+                CK(cudaMemcpyAsync(h_dst + out_spans[i].offset, ctx->io_out.as<uint8_t>() + out_spans[i].offset,
+                                   lens[i], cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < nblocks; i++) {
+        if (out_lens) out_lens[i] = lens[i];
+        if (status) status[i] = sts[i];
+    }
+    return first;
 }
 
 }  // extern "C"

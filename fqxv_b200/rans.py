@@ -121,6 +121,13 @@ def lib() -> ctypes.CDLL:
                                              u8p, u8p, ctypes.c_int]
         L.fqxv_rans_decode_batch.argtypes = [ctypes.c_void_p, u8p, u8p, sz, ctypes.c_uint64, u8p, u8p, u8p, u8p,
                                              ctypes.c_int]
+        L.fqxv_rans_encode_batch_host.argtypes = [ctypes.c_void_p, u8p, u8p, sz, ctypes.c_int, u8p,
+                                                  ctypes.c_uint64, u8p, u8p]
+        L.fqxv_rans_decode_batch_host.argtypes = [ctypes.c_void_p, u8p, u8p, sz, ctypes.c_uint64, u8p, u8p, u8p,
+                                                  u8p]
+        L.fqxv_rans_ctx_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.fqxv_rans_ctx_stage_stats.argtypes = [ctypes.c_void_p, u8p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.c_int]
         _lib = L
     return _lib
 

@@ -164,6 +164,32 @@ int fqxv_rans_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_
                            const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status,
                            int persistent);
 
+/* Host-buffer batch forms of the two calls above: the input arena is copied
+ * to the device, coded in one pass, and the results copied back (pinned host
+ * memory makes the copies asynchronous DMA). out_spans/out_lens/status as
+ * above; for encode, out_spans index into h_dst. */
+int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
+                                size_t nblocks, int order, uint8_t *h_dst, uint64_t dst_cap,
+                                fqxv_rans_span *out_spans, int32_t *out_orders);
+int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
+                                size_t nblocks, uint64_t max_len, uint8_t *h_dst,
+                                const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status);
+
+/* ---- per-stage device timing -------------------------------------------
+ * When enabled, every kernel launch of a context is bracketed by CUDA events
+ * on the context's stream and its duration accumulated per stage. Launch
+ * counts are kept whether or not timing is on. */
+typedef struct fqxv_rans_stage_stat {
+    char name[24];
+    uint64_t launches;
+    double ms;
+} fqxv_rans_stage_stat;
+
+int fqxv_rans_ctx_set_profiling(fqxv_rans_ctx *ctx, int on);
+/* Copies up to `cap` stage records into `out`, the count into *n; reset != 0
+ * clears the counters afterwards. */
+int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int cap, int *n, int reset);
+
 #ifdef __cplusplus
 }
 #endif
