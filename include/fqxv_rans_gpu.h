@@ -175,6 +175,21 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
                                 size_t nblocks, uint64_t max_len, uint8_t *h_dst,
                                 const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status);
 
+/* No counterpart in the reference. Encode one block that is already in device
+ * memory without allocating any device memory, for callers that cannot call
+ * cudaMalloc (a fixed device-memory budget reserved at start-up, an allocator
+ * that must not be re-entered, a process that forbids driver allocations once
+ * running). Its working memory is one file-scope device array of about 4.8 MiB
+ * that every GPU loading the library holds until exit. d_src holds n <= 1 MiB
+ * bytes (larger: FQXV_RANS_E_TOO_LARGE); the stream is written to d_dst, which
+ * must hold fqxv_rans_encode_bound(n, order) bytes; its length goes to
+ * *out_len. Work is queued on `stream` (a cudaStream_t, 0 = legacy default) and
+ * the call returns once it is done. All calls share the array: calls whose
+ * work overlaps on the GPU race and corrupt each other. The first call on a
+ * device looks up the array's address; make it before any stream capture. */
+int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int order, uint8_t *d_dst, size_t dst_cap,
+                             size_t *out_len, void *stream);
+
 /* ---- per-stage device timing -------------------------------------------
  * When enabled, every kernel launch of a context is bracketed by CUDA events
  * on the context's stream and its duration accumulated per stage. Launch
