@@ -16,7 +16,8 @@ from . import rans
 
 
 class StageStat(ctypes.Structure):
-    _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double)]
+    _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double),
+                ("bytes", ctypes.c_uint64)]
 
 
 def _spans(a) -> np.ndarray:
@@ -134,5 +135,5 @@ class Codec:
         n = ctypes.c_int(0)
         rans.raise_for(self._lib.fqxv_rans_ctx_stage_stats(self._h, ctypes.cast(arr, ctypes.c_void_p), 16,
                                                            ctypes.byref(n), 1 if reset else 0))
-        return {arr[i].name.decode(): {"launches": int(arr[i].launches), "ms": float(arr[i].ms)}
-                for i in range(n.value)}
+        return {arr[i].name.decode(): {"launches": int(arr[i].launches), "ms": float(arr[i].ms),
+                                       "bytes": int(arr[i].bytes)} for i in range(n.value)}

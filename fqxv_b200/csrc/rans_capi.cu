@@ -74,9 +74,12 @@ struct HostBuf {
     }
 };
 
-enum Stage { kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecRun, kStages };
-const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan",
-                                          "enc_pack", "dec_parse", "dec_run"};
+enum Stage {
+    kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
+    kStages
+};
+const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan", "enc_pack",
+                                          "dec_parse", "dec_o0", "dec_o1_dense", "dec_o1_global"};
 
 // CUDA-event brackets around each kernel launch on the context's stream.
 // Durations are collected after the call's final synchronisation.
@@ -90,6 +93,7 @@ struct StageTimer {
     std::vector<cudaEvent_t> pool;
     double ms[kStages] = {};
     uint64_t launches[kStages] = {};
+    uint64_t bytes[kStages] = {};   // algorithmic bytes moved by the stage's launches
     cudaEvent_t get() {
         if (!pool.empty()) {
             cudaEvent_t e = pool.back();
@@ -145,6 +149,8 @@ struct fqxv_rans_ctx {
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};   // decode classes run side by side
+    cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
     std::mutex mu;
     // encode
     DevBuf e_blocks, e_order, e_jobs, e_tbl, e_words, e_hist, e_misc;
@@ -318,6 +324,15 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     ctx->timer.collect();
     const EncBlock *rb = reinterpret_cast<const EncBlock *>(hs);
     for (size_t i = 0; i < nb; i++) {
+        // Algorithmic bytes per stage: the model reads the block, each encode
+        // job reads it and writes its words, the pack reads the chosen words
+        // and writes the stream.
+        ctx->timer.bytes[kStEncModel] += rb[i].n;
+        if (o0) ctx->timer.bytes[kStEncRun] += rb[i].n + 2 * rb[i].nwords[0];
+        if (o1) ctx->timer.bytes[kStEncRun] += rb[i].n + 2 * rb[i].nwords[1];
+        ctx->timer.bytes[kStEncPack] += 2 * rb[i].nwords[rb[i].chosen] + rb[i].out_size[rb[i].chosen];
+    }
+    for (size_t i = 0; i < nb; i++) {
         out_spans[i].offset = rb[i].out_off;
         out_spans[i].length = rb[i].out_size[rb[i].chosen];
         if (out_orders) out_orders[i] = rb[i].chosen;
@@ -363,25 +378,75 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     int *queue = ctx->d_misc.as<int>();
     CK(cudaMemsetAsync(queue, 0, 16, s));
     DecStream *dS = ctx->d_streams.as<DecStream>();
-    const uint32_t *dO = ctx->d_order.as<uint32_t>();
     uint8_t *dT = ctx->d_tbl.as<uint8_t>();
     if (persistent) {
         cudaEvent_t t0 = ctx->timer.begin(s);
         launch_dec_parse(d_src, dS, (int)nb, dT, (int)std::min<size_t>(nb, (size_t)ctx->sms * 8), s);
         ctx->timer.end(kStDecParse, t0, s);
-        t0 = ctx->timer.begin(s);
-        launch_dec_run(d_src, dS, dO, (int)nb, dT, d_dst, queue,
-                       (int)std::min<size_t>((nb + 3) / 4, (size_t)ctx->sms * 16), s);
-        ctx->timer.end(kStDecRun, t0, s);
     } else {
         for (size_t j = 0; j < nb; j++) {
-            CK(cudaMemsetAsync(queue, 0, 4, s));
             cudaEvent_t t0 = ctx->timer.begin(s);
             launch_dec_parse(d_src, dS + ord[j], 1, dT, 1, s);
             ctx->timer.end(kStDecParse, t0, s);
-            t0 = ctx->timer.begin(s);
-            launch_dec_run(d_src, dS, dO + j, 1, dT, d_dst, queue, 1, s);
-            ctx->timer.end(kStDecRun, t0, s);
+        }
+    }
+    CK(cudaGetLastError());
+    // The parse decides each stream's class (order-0, order-1 with shared-
+    // memory tables, order-1 with global tables); one kernel per class.
+    CK(cudaMemcpyAsync(hst, dS, szs, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    {
+        const DecStream *ps = reinterpret_cast<const DecStream *>(hst);
+        std::vector<uint32_t> lists[3];
+        uint32_t smem[3] = {0, 0, 0};
+        uint64_t cbytes[3] = {0, 0, 0};
+        for (uint32_t i : ord) {
+            const int c = ps[i].cls;
+            if (c < kClsO0 || c > kClsO1Global) continue;
+            lists[c - kClsO0].push_back(i);
+            smem[c - kClsO0] = std::max(smem[c - kClsO0], dec_smem_bytes(c, ps[i].nd));
+            cbytes[c - kClsO0] += ps[i].src_len + ps[i].n;
+        }
+        size_t tot = lists[0].size() + lists[1].size() + lists[2].size();
+        CK(ctx->d_order.ensure(std::max<size_t>(tot, 1) * 4, s));
+        uint32_t *hl = reinterpret_cast<uint32_t *>(hst + szs);
+        size_t at = 0, base[3];
+        for (int c = 0; c < 3; c++) {
+            base[c] = at;
+            std::memcpy(hl + at, lists[c].data(), lists[c].size() * 4);
+            at += lists[c].size();
+        }
+        if (tot) CK(cudaMemcpyAsync(ctx->d_order.p, hl, tot * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(queue, 0, 64, s));
+        CK(cudaEventRecord(ctx->ev_fork, s));
+        const uint32_t *dl = ctx->d_order.as<uint32_t>();
+        const int st_of[3] = {kStDecO0, kStDecO1Dense, kStDecO1Global};
+        for (int c = 0; c < 3; c++) {
+            const size_t m = lists[c].size();
+            if (!m) continue;
+            cudaStream_t as = ctx->aux[c];
+            CK(cudaStreamWaitEvent(as, ctx->ev_fork, 0));
+            const uint32_t sm_b = smem[c] + 2048;  // + static shared memory and per-CTA reserve
+            int per_sm = (int)(233472u / sm_b);
+            per_sm = std::max(1, std::min(per_sm, 32));
+            if (persistent) {
+                const int grid = (int)std::min<size_t>(m, (size_t)ctx->sms * per_sm);
+                cudaEvent_t t0 = ctx->timer.begin(as);
+                launch_dec_run(kClsO0 + c, d_src, dS, dl + base[c], (int)m, dT, d_dst, queue + 4 * c, grid,
+                               smem[c], as);
+                ctx->timer.end(st_of[c], t0, as);
+            } else {
+                for (size_t j = 0; j < m; j++) {
+                    CK(cudaMemsetAsync(queue + 4 * c, 0, 4, as));
+                    cudaEvent_t t0 = ctx->timer.begin(as);
+                    launch_dec_run(kClsO0 + c, d_src, dS, dl + base[c] + j, 1, dT, d_dst, queue + 4 * c, 1,
+                                   dec_smem_bytes(kClsO0 + c, ps[lists[c][j]].nd), as);
+                    ctx->timer.end(st_of[c], t0, as);
+                }
+            }
+            ctx->timer.bytes[st_of[c]] += cbytes[c];
+            CK(cudaEventRecord(ctx->ev_join[c], as));
+            CK(cudaStreamWaitEvent(s, ctx->ev_join[c], 0));
         }
     }
     CK(cudaGetLastError());
@@ -463,7 +528,12 @@ int fqxv_rans_ctx_create(int device, fqxv_rans_ctx **out) {
     auto *c = new fqxv_rans_ctx();
     c->device = device;
     c->sms = sm_count(device);
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < 3 && ok; i++)
+        ok = cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         cudaGetLastError();
         delete c;
         return FQXV_RANS_E_CUDA;
@@ -483,6 +553,11 @@ void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
     ctx->h_stage.release();
     ctx->h_io.release();
     ctx->timer.release();
+    for (int i = 0; i < 3; i++) {
+        if (ctx->aux[i]) cudaStreamDestroy(ctx->aux[i]);
+        if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -612,12 +687,14 @@ int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int
         std::strncpy(out[k].name, kStageNames[i], sizeof out[k].name - 1);
         out[k].launches = ctx->timer.launches[i];
         out[k].ms = ctx->timer.ms[i];
+        out[k].bytes = ctx->timer.bytes[i];
     }
     *n = k;
     if (reset) {
         for (int i = 0; i < kStages; i++) {
             ctx->timer.launches[i] = 0;
             ctx->timer.ms[i] = 0.0;
+            ctx->timer.bytes[i] = 0;
         }
     }
     return FQXV_RANS_OK;

@@ -2,14 +2,25 @@
 //
 //   1. dec_parse_kernel  one CTA per stream: header checks in the reference's
 //      order (lib.rs:226-231, scalar.rs:143-217, model.rs:160-205), then the
-//      decode tables: order-0 one packed word per slot ((f-1)<<20 | offset<<8
-//      | sym, the layout of avx2.rs:29-54); order-1 per present context a
-//      slot -> (symbol, dense next context) table and a (freq << 12 | cum)
-//      table.
-//   2. dec_run_kernel    one warp per stream from a device work queue: lane l
-//      owns state l; renorm words are handed out in stream order by a
-//      ballot/popc prefix over the lanes that need one. Order-1 resolves the
-//      previous-symbol context chain of each round lane by lane.
+//      decode tables in the table arena:
+//        order-0: one packed word per slot ((f-1)<<20 | offset<<8 | sym, the
+//                 layout of avx2.rs:29-54);
+//        order-1 dense: all contexts and symbols renumbered densely (|D| <= 47)
+//                 so that one u8 lookup chain[ctx][slot] gives the next
+//                 context, plus a (freq << 12 | cum) table per (ctx, sym);
+//        order-1 global: the same idea with u16 entries for larger alphabets.
+//   2. one decode kernel per class, one warp per CTA, streams taken from a
+//      device queue largest first. Lane l owns state l; renorm words are
+//      handed out in stream order by a ballot/popc prefix over the lanes that
+//      need one, read from a shared-memory ring that the warp refills with
+//      16-byte loads issued eight-plus rounds ahead. The stream's tables are
+//      staged into shared memory with one TMA bulk copy (cp.async.bulk +
+//      mbarrier, bounded wait).
+//      Order-1 resolves each round's context chain s_i = table[s_{i-1}][slot_i]
+//      in four segments of eight lanes: the first segment from the known
+//      context, the other three for every possible incoming context at once,
+//      then three dependent lookups pick the real paths (11 dependent shared
+//      memory reads per round instead of 32).
 // Malformed input never faults: every read of the stream is bounds checked
 // and errors are reported per stream as the reference's Malformed kinds.
 #include "rans_common.cuh"
@@ -17,14 +28,21 @@
 
 namespace fqxv {
 
+// ---------------------------------------------------------------------------
+// header parse and table build
+// ---------------------------------------------------------------------------
+
 __global__ void __launch_bounds__(kParseThreads)
     dec_parse_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams, int nstreams,
                      uint8_t *__restrict__ tbl) {
     __shared__ uint32_t sfreq[256];
     __shared__ uint32_t scum[257];
     __shared__ uint32_t wsum[kParseThreads / 32];
-    __shared__ uint8_t ctxmap[256];
-    __shared__ int s_k;
+    __shared__ uint8_t ctxmap[256];   // raw context -> present-table index (0xFF absent)
+    __shared__ uint8_t ctxlist[256];  // present-table index -> raw context
+    __shared__ uint8_t dmap[256];     // raw byte -> dense index (0xFF not in D)
+    __shared__ uint8_t symseen[256];
+    __shared__ int s_k, s_nd;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     for (int si = blockIdx.x; si < nstreams; si += gridDim.x) {
@@ -46,6 +64,10 @@ __global__ void __launch_bounds__(kParseThreads)
             S.n = (status == FQXV_RANS_OK) ? n : 0;
             S.nctx = 0;
             S.ctx0 = 0xff;
+            S.cls = kClsNone;
+            S.nd = 0;
+            S.start = 0;
+            S.tbl_bytes = 0;
         }
         if (status != FQXV_RANS_OK || n == 0) {
             if (tid == 0) S.status = status;
@@ -53,8 +75,8 @@ __global__ void __launch_bounds__(kParseThreads)
             continue;
         }
         uint8_t *T = tbl + S.tbl_off;
-        // Validate one 256-entry frequency table at byte offset `at` (the
-        // caller checked it is in bounds); fills sfreq/scum. model.rs:160-174.
+        // Read one 256-entry frequency table at byte offset `at` (in bounds)
+        // into sfreq/scum and validate it (model.rs:160-174).
         auto load_table = [&](uint64_t at) -> int {
             const uint32_t f = tid < 256 ? (uint32_t)p[at + 2 * tid] | ((uint32_t)p[at + 2 * tid + 1] << 8) : 0u;
             if (tid < 256) sfreq[tid] = f;
@@ -68,9 +90,19 @@ __global__ void __launch_bounds__(kParseThreads)
             for (int w = 0; w < kParseThreads / 32; w++) tot += wsum[w];
             if (tid == 0) scum[256] = tot;
             __syncthreads();
-            // Running sums are monotone, so "some prefix exceeds" == "total exceeds".
+            // Running sums are monotone: "some prefix exceeds" == "total exceeds".
             return tot > kTotFreq ? FQXV_RANS_E_FREQ_EXCEEDS
                                   : (tot != kTotFreq ? FQXV_RANS_E_FREQ_SUM : FQXV_RANS_OK);
+        };
+        // Symbol of `slot` in the table held in sfreq/scum: the largest s with
+        // cum[s] <= slot (which always has f[s] > 0 in a valid table).
+        auto slot_sym = [&](uint32_t slot) -> int {
+            int lo = 0, hi = 255;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (scum[mid] <= slot) lo = mid; else hi = mid - 1;
+            }
+            return lo;
         };
         uint64_t hdr = 0;
         if (order == 0) {
@@ -82,67 +114,130 @@ __global__ void __launch_bounds__(kParseThreads)
             if (status == FQXV_RANS_OK) {
                 uint32_t *P = reinterpret_cast<uint32_t *>(T);
                 for (int slot = tid; slot < (int)kTotFreq; slot += blockDim.x) {
-                    // largest s with cum[s] <= slot and f[s] > 0
-                    int lo = 0, hi = 255;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (scum[mid] <= (uint32_t)slot) lo = mid; else hi = mid - 1;
-                    }
-                    const uint32_t f = sfreq[lo], c = scum[lo];
-                    P[slot] = ((f - 1) << 20) | (((uint32_t)slot - c) << 8) | (uint32_t)lo;
+                    const int s = slot_sym((uint32_t)slot);
+                    P[slot] = ((sfreq[s] - 1) << 20) | (((uint32_t)slot - scum[s]) << 8) | (uint32_t)s;
+                }
+                if (tid == 0) {
+                    S.cls = kClsO0;
+                    S.tbl_bytes = 16384;
                 }
             }
+        } else if (L < kHdr + kO1Bitmap) {
+            status = FQXV_RANS_E_TRUNCATED;
         } else {
-            if (L < kHdr + kO1Bitmap) {
-                status = FQXV_RANS_E_TRUNCATED;
-            } else {
+            if (warp == 0) {
+                const uint32_t byte = p[kHdr + lane];
+                const uint32_t c = __popc(byte);
+                uint32_t base = warp_incl_scan(c) - c;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int ctx = lane * 8 + k;
+                    if ((byte >> k) & 1u) {
+                        ctxlist[base] = (uint8_t)ctx;
+                        ctxmap[ctx] = (uint8_t)(base++);
+                    } else {
+                        ctxmap[ctx] = 0xff;
+                    }
+                }
+                if (lane == 31) s_k = (int)base;
+            }
+            if (tid < 256) symseen[tid] = 0;
+            __syncthreads();
+            const int K = s_k;
+            // Pass 1: every table in ascending context order -- truncation and
+            // validity are reported for the first failing table (scalar.rs:186-194).
+            for (int t = 0; t < K; t++) {
+                const uint64_t at = kHdr + kO1Bitmap + kO1Table * (uint64_t)t;
+                if (L < at + kO1Table) {
+                    status = FQXV_RANS_E_TRUNCATED;
+                    break;
+                }
+                status = load_table(at);
+                if (status != FQXV_RANS_OK) break;
+                if (tid < 256 && sfreq[tid]) symseen[tid] = 1;
+                __syncthreads();
+            }
+            hdr = kHdr + kO1Bitmap + kO1Table * (uint64_t)K;
+            if (status == FQXV_RANS_OK && L < hdr + kStatesBytes) status = FQXV_RANS_E_TRUNCATED;
+            if (status == FQXV_RANS_OK && n > S.dst_cap) status = FQXV_RANS_E_ALLOC;
+            if (status == FQXV_RANS_OK) {
+                // D = present contexts plus every symbol of their tables.
                 if (warp == 0) {
-                    const uint32_t byte = p[kHdr + lane];
-                    const uint32_t c = __popc(byte);
-                    uint32_t base = warp_incl_scan(c) - c;
+                    uint32_t flags = 0;
 #pragma unroll
                     for (int k = 0; k < 8; k++) {
-                        const int ctx = lane * 8 + k;
-                        if ((byte >> k) & 1u) {
-                            ctxmap[ctx] = (uint8_t)(base++);
-                        } else {
-                            ctxmap[ctx] = 0xff;
-                        }
+                        const int s = lane * 8 + k;
+                        if (symseen[s] || ctxmap[s] != 0xff) flags |= 1u << k;
                     }
-                    if (lane == 31) s_k = (int)base;
+                    const uint32_t c = __popc(flags);
+                    uint32_t base = warp_incl_scan(c) - c;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) dmap[lane * 8 + k] = (flags >> k) & 1u ? (uint8_t)(base++) : 0xff;
+                    if (lane == 31) s_nd = (int)base;
                 }
                 __syncthreads();
-                const int K = s_k;
-                if (tid < 256) T[kDecCtxMap + tid] = ctxmap[tid];
-                for (int t = 0; t < K && status == FQXV_RANS_OK; t++) {
-                    const uint64_t at = kHdr + kO1Bitmap + kO1Table * (uint64_t)t;
-                    if (L < at + kO1Table) {
-                        status = FQXV_RANS_E_TRUNCATED;
-                        break;
-                    }
-                    status = load_table(at);
-                    if (status != FQXV_RANS_OK) break;
-                    uint8_t *C = T + kDecO1Base + kDecO1Ctx * (uint64_t)t;
-                    uint16_t *S16 = reinterpret_cast<uint16_t *>(C);
-                    uint32_t *FC = reinterpret_cast<uint32_t *>(C + kDecO1Slot);
-                    if (tid < 256) FC[tid] = (sfreq[tid] << kScaleBits) | scum[tid];
-                    for (int slot = tid; slot < (int)kTotFreq; slot += blockDim.x) {
-                        int lo = 0, hi = 255;
-                        while (lo < hi) {
-                            const int mid = (lo + hi + 1) >> 1;
-                            if (scum[mid] <= (uint32_t)slot) lo = mid; else hi = mid - 1;
+                const int nd = s_nd;
+                if (nd <= kDenseMax) {
+                    const int dead = nd;
+                    const int stride = nd + 1;
+                    uint8_t *CT = T;
+                    uint32_t *FC = reinterpret_cast<uint32_t *>(T + (uint64_t)stride * 4096);
+                    uint8_t *DS = T + (uint64_t)stride * 4096 + dense_fc_bytes(nd);
+                    // Rows of dense indices without a table (and DEAD) map every
+                    // slot to DEAD; the FC table starts zeroed.
+                    for (int b = 0; b <= 256; b++) {
+                        int d;
+                        if (b < 256) {
+                            if (dmap[b] == 0xff || ctxmap[b] != 0xff) continue;
+                            d = dmap[b];
+                        } else {
+                            d = dead;
                         }
-                        S16[slot] = (uint16_t)(((uint32_t)lo << 8) | ctxmap[lo]);
+                        uint32_t *row = reinterpret_cast<uint32_t *>(CT + (uint64_t)d * 4096);
+                        const uint32_t v = 0x01010101u * (uint32_t)dead;
+                        for (int i = tid; i < 1024; i += blockDim.x) row[i] = v;
                     }
+                    for (int i = tid; i < stride * stride; i += blockDim.x) FC[i] = 0;
+                    if (tid < 256 && dmap[tid] != 0xff) DS[dmap[tid]] = (uint8_t)tid;
                     __syncthreads();
+                    // Pass 2: chain rows and FC rows of the present contexts.
+                    for (int t = 0; t < K; t++) {
+                        load_table(kHdr + kO1Bitmap + kO1Table * (uint64_t)t);
+                        const int dc = dmap[ctxlist[t]];
+                        uint8_t *row = CT + (uint64_t)dc * 4096;
+                        for (int slot = tid; slot < (int)kTotFreq; slot += blockDim.x)
+                            row[slot] = dmap[slot_sym((uint32_t)slot)];
+                        if (tid < 256 && sfreq[tid])
+                            FC[dc * stride + dmap[tid]] = (sfreq[tid] << kScaleBits) | scum[tid];
+                        __syncthreads();
+                    }
+                    if (tid == 0) {
+                        S.cls = kClsO1Dense;
+                        S.nd = nd;
+                        S.start = dmap[0] != 0xff ? dmap[0] : dead;
+                        S.tbl_bytes = dense_table_bytes(nd);
+                    }
+                } else {
+                    if (tid < 256) T[kDecCtxMap + tid] = ctxmap[tid];
+                    for (int t = 0; t < K; t++) {
+                        load_table(kHdr + kO1Bitmap + kO1Table * (uint64_t)t);
+                        uint8_t *C = T + kDecO1Base + kDecO1Ctx * (uint64_t)t;
+                        uint16_t *S16 = reinterpret_cast<uint16_t *>(C);
+                        uint32_t *FCg = reinterpret_cast<uint32_t *>(C + kDecO1Slot);
+                        if (tid < 256) FCg[tid] = (sfreq[tid] << kScaleBits) | scum[tid];
+                        for (int slot = tid; slot < (int)kTotFreq; slot += blockDim.x) {
+                            const int s = slot_sym((uint32_t)slot);
+                            S16[slot] = (uint16_t)(((uint32_t)s << 8) | ctxmap[s]);
+                        }
+                        __syncthreads();
+                    }
+                    if (tid == 0) {
+                        S.cls = kClsO1Global;
+                        S.nd = nd;
+                        S.ctx0 = ctxmap[0];
+                    }
                 }
-                hdr = kHdr + kO1Bitmap + kO1Table * (uint64_t)K;
-                if (status == FQXV_RANS_OK && L < hdr + kStatesBytes) status = FQXV_RANS_E_TRUNCATED;
-                if (status == FQXV_RANS_OK && n > S.dst_cap) status = FQXV_RANS_E_ALLOC;
-                if (tid == 0) {
-                    S.nctx = K;
-                    S.ctx0 = ctxmap[0];
-                }
+                if (tid == 0) S.nctx = K;
             }
         }
         if (status == FQXV_RANS_OK && tid < kStates) S.states[tid] = ld_u32_le(p + hdr + 4 * tid);
@@ -150,6 +245,7 @@ __global__ void __launch_bounds__(kParseThreads)
             // The renorm words follow the 32 states (scalar.rs:130-140).
             const uint64_t wbeg = hdr + kStatesBytes;
             S.status = status;
+            if (status != FQXV_RANS_OK) S.cls = kClsNone;
             S.words_off = S.src_off + wbeg;
             S.words_len = L > wbeg ? L - wbeg : 0;
         }
@@ -157,19 +253,134 @@ __global__ void __launch_bounds__(kParseThreads)
     }
 }
 
+// ---------------------------------------------------------------------------
+// shared pieces of the decode kernels
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
 __device__ __forceinline__ uint32_t load_word(const uint8_t *__restrict__ w, uint64_t j) {
     return (uint32_t)__ldg(w + 2 * j) | ((uint32_t)__ldg(w + 2 * j + 1) << 8);
 }
 
+// TMA bulk copy of a table image into shared memory, completion tracked by an
+// mbarrier; the wait is bounded and reports failure instead of hanging.
+struct TableStager {
+    uint64_t *bar;
+    uint32_t phase;
+
+    __device__ void init(uint64_t *b) {
+        bar = b;
+        phase = 0;
+        if ((threadIdx.x & 31) == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncwarp();
+    }
+    // bytes and both addresses are multiples of 16.
+    __device__ void issue(void *dst, const void *src, uint32_t bytes) {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                         "r"(bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(dst)),
+                "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                : "memory");
+        }
+    }
+    __device__ bool wait() {
+        uint32_t done = 0;
+        for (uint32_t it = 0; it < (1u << 22) && !done; it++) {
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                : "=r"(done)
+                : "r"(smem_u32(bar)), "r"(phase)
+                : "memory");
+        }
+        phase ^= 1u;
+        __syncwarp();
+        return __all_sync(0xffffffffu, done != 0);
+    }
+};
+
+// Renorm-word ring: 4 segments of 512 bytes of the word region (16-byte
+// aligned chunks, so a segment is one 16-byte load per lane). Segment q holds
+// bytes [abase + 512 q, +512). Three segments are resident and a fourth is in
+// flight in registers; it is stored when the read position enters the
+// segment after the oldest, i.e. more than eight rounds before it is needed.
+struct WordRing {
+    const uint8_t *abase;   // 16-byte aligned start, <= first word byte
+    const uint8_t *words;   // first word byte
+    uint64_t avail;         // bytes from abase to the end of the region
+    uint32_t lead;          // words - abase
+    uint64_t next_seg;      // next segment to store
+    uint4 pend;             // this lane's 16 bytes of segment next_seg
+    uint8_t *ring;
+
+    __device__ __forceinline__ uint4 fetch(uint64_t q) const {
+        const uint64_t rel = 512 * q + 16 * (threadIdx.x & 31);
+        if (rel < avail) return __ldg(reinterpret_cast<const uint4 *>(abase + rel));
+        return make_uint4(0, 0, 0, 0);
+    }
+    __device__ __forceinline__ void put(uint64_t q, uint4 v) {
+        *reinterpret_cast<uint4 *>(ring + ((512 * q + 16 * (threadIdx.x & 31)) & (kRingBytes - 1))) = v;
+    }
+    __device__ void reset(uint64_t q0) {
+        __syncwarp();
+        const uint4 a = fetch(q0), b = fetch(q0 + 1), c = fetch(q0 + 2);
+        pend = fetch(q0 + 3);
+        put(q0, a);
+        put(q0 + 1, b);
+        put(q0 + 2, c);
+        next_seg = q0 + 3;
+        __syncwarp();
+    }
+    __device__ void init(const uint8_t *w, uint64_t len, uint8_t *r) {
+        words = w;
+        abase = reinterpret_cast<const uint8_t *>((uintptr_t)w & ~(uintptr_t)15);
+        lead = (uint32_t)(w - abase);
+        avail = lead + len;
+        ring = r;
+        reset(0);
+    }
+    // Keep [pos, pos + 64) resident for the word index wp (warp-uniform).
+    __device__ __forceinline__ void advance(uint64_t wp) {
+        const uint64_t pos = lead + 2 * wp;
+        while (pos >= 512 * (next_seg - 3)) {
+            if (pos >= 512 * (next_seg - 2)) {
+                reset(pos / 512);  // a jump of more than one segment
+                return;
+            }
+            __syncwarp();
+            put(next_seg, pend);
+            next_seg++;
+            pend = fetch(next_seg);
+            __syncwarp();
+        }
+    }
+    __device__ __forceinline__ uint32_t word(uint64_t j) const {
+        const uint64_t rel = lead + 2 * j;
+        return (uint32_t)ring[rel & (kRingBytes - 1)] | ((uint32_t)ring[(rel + 1) & (kRingBytes - 1)] << 8);
+    }
+};
+
 // Renormalise the lanes in `need` (the reference's `while v < RANS_L`,
 // scalar.rs:233-235). Fast path: every needing lane takes exactly one word,
-// lane order = stream order. A lane whose value is 0 needs more than one word
-// (only malformed streams do this); the round is then replayed lane by lane.
-// Returns false on running out of words (scalar.rs:261, "truncated stream").
-__device__ __forceinline__ bool renorm_round(uint32_t &v, bool need, const uint8_t *__restrict__ wb,
-                                             uint64_t &wp, uint64_t navail, uint32_t lt) {
+// lane order = stream order, from the ring. A lane whose value is 0 needs more
+// than one word (only malformed streams do this); the round is then replayed
+// lane by lane from global memory. Returns false when the words run out
+// (scalar.rs:261, "truncated stream").
+__device__ __forceinline__ bool renorm_round(uint32_t &v, bool need, const WordRing &R, uint64_t &wp,
+                                             uint64_t navail, uint32_t lt) {
     const int lane = threadIdx.x & 31;
-    const uint32_t cand = (wp + lane < navail) ? load_word(wb, wp + lane) : 0u;
+    const uint32_t cand = (wp + lane < navail) ? R.word(wp + lane) : 0u;
     const uint32_t mask = __ballot_sync(0xffffffffu, need);
     if (__any_sync(0xffffffffu, need && v == 0)) {
         uint64_t wpl = wp;
@@ -182,7 +393,7 @@ __device__ __forceinline__ bool renorm_round(uint32_t &v, bool need, const uint8
                         ok = false;
                         break;
                     }
-                    vv = (vv << 16) | load_word(wb, wpl++);
+                    vv = (vv << 16) | load_word(R.words, wpl++);
                 }
                 v = vv;
             }
@@ -201,112 +412,277 @@ __device__ __forceinline__ bool renorm_round(uint32_t &v, bool need, const uint8
     return true;
 }
 
-// scalar.rs:157-178 / avx512.rs:78-134: order-0 decode of one stream.
-__device__ __forceinline__ int decode_o0(const DecStream &S, const uint32_t *__restrict__ P,
-                                         const uint8_t *__restrict__ src, uint8_t *__restrict__ out) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t lt = lanemask_lt();
-    const uint64_t n = S.n;
-    uint32_t x = S.states[lane];
-    const uint8_t *wb = src + S.words_off;
-    const uint64_t navail = S.words_len / 2;
-    uint64_t wp = 0;
-    const uint64_t R = (n + 31) / 32;
-    for (uint64_t r = 0; r < R; r++) {
-        const uint64_t i = r * 32 + lane;
-        const bool active = i < n;
-        if ((r & 7) == 0 && lane == 0 && wp + 512 < navail)
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(wb + 2 * (wp + 512)));
-        const uint32_t e = __ldg(P + (x & (kTotFreq - 1)));
-        uint32_t v = ((e >> 20) + 1) * (x >> kScaleBits) + ((e >> 8) & 0xfffu);
-        const bool need = active && v < kRansL;
-        if (!renorm_round(v, need, wb, wp, navail, lt)) return FQXV_RANS_E_TRUNCATED;
-        if (active) {
-            out[i] = (uint8_t)e;
-            x = v;
-        }
-    }
-    return FQXV_RANS_OK;
+__device__ __forceinline__ int pop_job(int *queue) {
+    int j = 0;
+    if ((threadIdx.x & 31) == 0) j = atomicAdd(queue, 1);
+    return __shfl_sync(0xffffffffu, j, 0);
 }
 
-// scalar.rs:180-217: order-1 decode. Each round resolves the context chain
-// s_i = slot2sym[s_{i-1}][slot_i] lane by lane (the table lookups of a round
-// are dependent), then all lanes advance their states together.
-__device__ __forceinline__ int decode_o1(const DecStream &S, const uint8_t *__restrict__ T,
-                                         const uint8_t *__restrict__ src, uint8_t *__restrict__ out) {
-    const int lane = threadIdx.x & 31;
+// ---------------------------------------------------------------------------
+// order-0 (scalar.rs:157-178, avx512.rs:78-134)
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32)
+    dec_o0_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
+                  const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
+                  uint8_t *__restrict__ dst, int *__restrict__ queue) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    __shared__ __align__(8) uint64_t bar;
+    const int lane = threadIdx.x;
     const uint32_t lt = lanemask_lt();
-    const uint64_t n = S.n;
-    uint32_t x = S.states[lane];
-    const uint8_t *wb = src + S.words_off;
-    const uint64_t navail = S.words_len / 2;
-    const bool all_present = S.nctx == 256;
-    const uint8_t *base = T + kDecO1Base;
-    uint64_t wp = 0;
-    uint32_t t = (uint32_t)S.ctx0;
-    const uint64_t R = (n + 31) / 32;
-    for (uint64_t r = 0; r < R; r++) {
-        const uint64_t i = r * 32 + lane;
-        const bool active = i < n;
-        const uint64_t left = n - r * 32;
-        const int jmax = left < 32 ? (int)left : 32;
-        if ((r & 7) == 0 && lane == 0 && wp + 512 < navail)
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(wb + 2 * (wp + 512)));
-        const uint32_t slot = x & (kTotFreq - 1);
-        uint32_t my_t = 0, my_e = 0;
-        int absent_at = 32;
-#pragma unroll
-        for (int j = 0; j < 32; j++) {
-            const uint32_t sl = __shfl_sync(0xffffffffu, slot, j);
-            if (j < jmax) {
-                if (!all_present && t == 0xffu) {
-                    absent_at = j;
-                    break;
-                }
-                const uint32_t e16 = __ldg(reinterpret_cast<const uint16_t *>(base + kDecO1Ctx * t) + sl);
-                if (lane == j) {
-                    my_t = t;
-                    my_e = e16;
-                }
-                t = e16 & 0xffu;
+    uint32_t *P = reinterpret_cast<uint32_t *>(sm);
+    TableStager st;
+    st.init(&bar);
+    for (;;) {
+        const int j = pop_job(queue);
+        if (j >= nlist) return;
+        DecStream &S = streams[list[j]];
+        st.issue(P, tbl + S.tbl_off, 16384);
+        WordRing R;
+        R.init(src + S.words_off, S.words_len, sm + 16384);
+        if (!st.wait()) {
+            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
+            st.wait();
+            return;
+        }
+        const uint64_t n = S.n;
+        const uint64_t navail = S.words_len / 2;
+        uint32_t x = S.states[lane];
+        uint8_t *out = dst + S.dst_off;
+        uint64_t wp = 0;
+        int status = FQXV_RANS_OK;
+        const uint64_t rounds = (n + 31) / 32;
+        for (uint64_t r = 0; r < rounds; r++) {
+            R.advance(wp);
+            const uint64_t i = r * 32 + lane;
+            const bool active = i < n;
+            const uint32_t e = P[x & (kTotFreq - 1)];
+            uint32_t v = ((e >> 20) + 1) * (x >> kScaleBits) + ((e >> 8) & 0xfffu);
+            const bool need = active && v < kRansL;
+            if (!renorm_round(v, need, R, wp, navail, lt)) {
+                status = FQXV_RANS_E_TRUNCATED;
+                break;
+            }
+            if (active) {
+                out[i] = (uint8_t)e;
+                x = v;
             }
         }
-        const bool valid = active && lane < absent_at;
-        uint32_t v = 0;
-        if (valid) {
-            const uint32_t sym = my_e >> 8;
-            const uint32_t fc = __ldg(reinterpret_cast<const uint32_t *>(base + kDecO1Ctx * my_t + kDecO1Slot) + sym);
-            v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
-        }
-        const bool need = valid && v < kRansL;
-        if (!renorm_round(v, need, wb, wp, navail, lt)) return FQXV_RANS_E_TRUNCATED;
-        if (absent_at < jmax) return FQXV_RANS_E_ABSENT_CONTEXT;
-        if (active) {
-            out[i] = (uint8_t)(my_e >> 8);
-            x = v;
-        }
+        if (lane == 0) S.status = status;
+        __syncwarp();
     }
-    return FQXV_RANS_OK;
 }
 
-__global__ void __launch_bounds__(kDecWarpsPerCta * 32)
-    dec_run_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
-                   const uint32_t *__restrict__ order, int nstreams, const uint8_t *__restrict__ tbl,
-                   uint8_t *__restrict__ dst, int *__restrict__ queue) {
-    const int lane = threadIdx.x & 31;
+// ---------------------------------------------------------------------------
+// order-1, dense tables in shared memory (scalar.rs:180-217)
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32)
+    dec_o1d_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
+                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
+                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(16) uint16_t s_slot[32];
+    __shared__ __align__(8) uint64_t s_out[kOutRows];
+    const int lane = threadIdx.x;
+    const uint32_t lt = lanemask_lt();
+    TableStager st;
+    st.init(&bar);
     for (;;) {
-        int j = 0;
-        if (lane == 0) j = atomicAdd(queue, 1);
-        j = __shfl_sync(0xffffffffu, j, 0);
-        if (j >= nstreams) return;
-        DecStream &S = streams[order[j]];
-        if (S.status != FQXV_RANS_OK || S.n == 0) continue;
-        const uint8_t *T = tbl + S.tbl_off;
+        const int j = pop_job(queue);
+        if (j >= nlist) return;
+        DecStream &S = streams[list[j]];
+        const int nd = S.nd;
+        const uint32_t dead = (uint32_t)nd;
+        const uint32_t stride = (uint32_t)nd + 1;
+        st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
+        WordRing R;
+        R.init(src + S.words_off, S.words_len, sm + ring_off);
+        // Chain tasks of this lane: task 0 = segment 0 from the known context;
+        // task 1 + (k - 1) * nd + c = segment k (1..3) entered with context c.
+        const int ntask = 1 + 3 * nd;
+        int seg_q[5], c_q[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            const int t = lane + 32 * q;
+            seg_q[q] = t == 0 ? 0 : (t < ntask ? 1 + (t - 1) / nd : -1);
+            c_q[q] = t == 0 ? 0 : (t < ntask ? (t - 1) % nd : 0);
+        }
+        if (!st.wait()) {
+            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
+            st.wait();
+            return;
+        }
+        const uint8_t *CT = sm;
+        const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + stride * 4096);
+        const uint8_t *DS = sm + stride * 4096 + dense_fc_bytes(nd);
+        const uint64_t deadrow = 0x0101010101010101ull * dead;
+        const uint64_t n = S.n;
+        const uint64_t navail = S.words_len / 2;
+        uint32_t x = S.states[lane];
         uint8_t *out = dst + S.dst_off;
-        const int st = S.order == 0 ? decode_o0(S, reinterpret_cast<const uint32_t *>(T), src, out)
-                                    : decode_o1(S, T, src, out);
-        if (lane == 0) S.status = st;
+        uint64_t wp = 0;
+        uint32_t din = (uint32_t)S.start;
+        int status = FQXV_RANS_OK;
+        const uint64_t rounds = (n + 31) / 32;
+        const int seg = lane >> 3, pos = lane & 7;
+        for (uint64_t r = 0; r < rounds; r++) {
+            R.advance(wp);
+            const uint64_t i = r * 32 + lane;
+            const bool active = i < n;
+            const uint32_t slot = x & (kTotFreq - 1);
+            s_slot[lane] = (uint16_t)slot;
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                if (seg_q[q] >= 0) {
+                    const uint4 sv = *reinterpret_cast<const uint4 *>(s_slot + 8 * seg_q[q]);
+                    const uint32_t sl[8] = {sv.x & 0xffffu, sv.x >> 16, sv.y & 0xffffu, sv.y >> 16,
+                                            sv.z & 0xffffu, sv.z >> 16, sv.w & 0xffffu, sv.w >> 16};
+                    uint32_t d = (lane == 0 && q == 0) ? din : (uint32_t)c_q[q];
+                    uint64_t row = 0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        d = CT[(d << 12) | sl[k]];
+                        row |= (uint64_t)d << (8 * k);
+                    }
+                    const int idx = (lane == 0 && q == 0) ? 0 : 1 + (seg_q[q] - 1) * nd + c_q[q];
+                    s_out[idx] = row;
+                }
+            }
+            __syncwarp();
+            const uint64_t r0 = s_out[0];
+            const uint32_t c1 = (uint32_t)(r0 >> 56);
+            const uint64_t r1 = c1 == dead ? deadrow : s_out[1 + c1];
+            const uint32_t c2 = (uint32_t)(r1 >> 56);
+            const uint64_t r2 = c2 == dead ? deadrow : s_out[1 + nd + c2];
+            const uint32_t c3 = (uint32_t)(r2 >> 56);
+            const uint64_t r3 = c3 == dead ? deadrow : s_out[1 + 2 * nd + c3];
+            const uint64_t row = seg == 0 ? r0 : seg == 1 ? r1 : seg == 2 ? r2 : r3;
+            const uint32_t in = seg == 0 ? din : seg == 1 ? c1 : seg == 2 ? c2 : c3;
+            const uint32_t d = (uint32_t)(row >> (8 * pos)) & 0xffu;
+            const uint32_t ctx = pos == 0 ? in : (uint32_t)(row >> (8 * pos - 8)) & 0xffu;
+            din = (uint32_t)(r3 >> 56);
+            __syncwarp();
+            // A lane whose context has no table reads DEAD (scalar.rs:204-206).
+            const uint32_t deadmask = __ballot_sync(0xffffffffu, active && d == dead);
+            const int absent_at = deadmask ? __ffs(deadmask) - 1 : 32;
+            const bool valid = active && lane < absent_at;
+            uint32_t v = 0;
+            if (valid) {
+                const uint32_t fc = FC[ctx * stride + d];
+                v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
+            }
+            const bool need = valid && v < kRansL;
+            if (!renorm_round(v, need, R, wp, navail, lt)) {
+                status = FQXV_RANS_E_TRUNCATED;
+                break;
+            }
+            if (absent_at < 32) {
+                status = FQXV_RANS_E_ABSENT_CONTEXT;
+                break;
+            }
+            if (active) {
+                out[i] = DS[d];
+                x = v;
+            }
+        }
+        if (lane == 0) S.status = status;
         __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// order-1, large alphabets: tables stay in global memory (L2), one dependent
+// lookup per position.
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(32)
+    dec_o1g_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
+                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
+                   uint8_t *__restrict__ dst, int *__restrict__ queue) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    const int lane = threadIdx.x;
+    const uint32_t lt = lanemask_lt();
+    for (;;) {
+        const int j = pop_job(queue);
+        if (j >= nlist) return;
+        DecStream &S = streams[list[j]];
+        const uint8_t *base = tbl + S.tbl_off + kDecO1Base;
+        WordRing R;
+        R.init(src + S.words_off, S.words_len, sm);
+        const uint64_t n = S.n;
+        const uint64_t navail = S.words_len / 2;
+        const bool all_present = S.nctx == 256;
+        uint32_t x = S.states[lane];
+        uint8_t *out = dst + S.dst_off;
+        uint64_t wp = 0;
+        uint32_t t = (uint32_t)S.ctx0;
+        int status = FQXV_RANS_OK;
+        const uint64_t rounds = (n + 31) / 32;
+        for (uint64_t r = 0; r < rounds; r++) {
+            R.advance(wp);
+            const uint64_t i = r * 32 + lane;
+            const bool active = i < n;
+            const uint64_t left = n - r * 32;
+            const int jmax = left < 32 ? (int)left : 32;
+            const uint32_t slot = x & (kTotFreq - 1);
+            uint32_t my_t = 0, my_e = 0;
+            int absent_at = 32;
+#pragma unroll
+            for (int k = 0; k < 32; k++) {
+                const uint32_t sl = __shfl_sync(0xffffffffu, slot, k);
+                if (k < jmax) {
+                    if (!all_present && t == 0xffu) {
+                        absent_at = k;
+                        break;
+                    }
+                    const uint32_t e16 = __ldg(reinterpret_cast<const uint16_t *>(base + kDecO1Ctx * t) + sl);
+                    if (lane == k) {
+                        my_t = t;
+                        my_e = e16;
+                    }
+                    t = e16 & 0xffu;
+                }
+            }
+            const bool valid = active && lane < absent_at;
+            uint32_t v = 0;
+            if (valid) {
+                const uint32_t sym = my_e >> 8;
+                const uint32_t fc =
+                    __ldg(reinterpret_cast<const uint32_t *>(base + kDecO1Ctx * my_t + kDecO1Slot) + sym);
+                v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
+            }
+            const bool need = valid && v < kRansL;
+            if (!renorm_round(v, need, R, wp, navail, lt)) {
+                status = FQXV_RANS_E_TRUNCATED;
+                break;
+            }
+            if (absent_at < jmax) {
+                status = FQXV_RANS_E_ABSENT_CONTEXT;
+                break;
+            }
+            if (active) {
+                out[i] = (uint8_t)(my_e >> 8);
+                x = v;
+            }
+        }
+        if (lane == 0) S.status = status;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+uint32_t dec_smem_bytes(int cls, int nd) {
+    switch (cls) {
+        case kClsO0: return 16384 + kRingBytes;
+        case kClsO1Dense: return (uint32_t)align_up(dense_table_bytes(nd), 128) + kRingBytes;
+        case kClsO1Global: return kRingBytes;
+        default: return 0;
     }
 }
 
@@ -316,10 +692,27 @@ void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint
     dec_parse_kernel<<<grid, kParseThreads, 0, s>>>(src, streams, nstreams, tbl);
 }
 
-void launch_dec_run(const uint8_t *src, DecStream *streams, const uint32_t *order, int nstreams,
-                    const uint8_t *tbl, uint8_t *dst, int *queue, int grid, cudaStream_t s) {
-    if (nstreams <= 0) return;
-    dec_run_kernel<<<grid, kDecWarpsPerCta * 32, 0, s>>>(src, streams, order, nstreams, tbl, dst, queue);
+void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
+                    const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
+                    cudaStream_t s) {
+    if (nlist <= 0 || grid <= 0) return;
+    switch (cls) {
+        case kClsO0:
+            cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+            dec_o0_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
+            break;
+        case kClsO1Dense:
+            cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+            dec_o1d_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
+                                                        smem_bytes - kRingBytes);
+            break;
+        case kClsO1Global:
+            cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+            dec_o1g_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
+            break;
+        default:
+            break;
+    }
 }
 
 }  // namespace fqxv

@@ -70,20 +70,39 @@ struct DecStream {
     uint64_t max_len;            // decode_bounded bound (UINT64_MAX: none)
     uint64_t n;                  // declared output length
     uint64_t words_off;          // absolute byte offset of the renorm words
-    uint64_t words_len;          // bytes after the header
+    uint64_t words_len;          // bytes after the states
     uint64_t tbl_off;            // table arena offset (bytes)
     int32_t order;
     int32_t status;
-    int32_t nctx;
-    int32_t ctx0;                // dense index of context 0 (0xFF: absent)
+    int32_t nctx;                // present order-1 contexts (K)
+    int32_t ctx0;                // global format: dense index of context 0 (0xFF: absent)
+    int32_t cls;                 // decode class (kClsO0, kClsO1Dense, kClsO1Global)
+    int32_t nd;                  // dense format: |D| (symbols and contexts), DEAD = nd
+    int32_t start;               // dense format: index of context 0 (DEAD when absent)
+    uint32_t tbl_bytes;          // bytes of the table image staged into shared memory
     uint32_t states[kStates];
 };
 
-// Decode table arena per stream (bytes from tbl_off):
-//   order-0: 4096 x u32 packed ((freq - 1) << 20) | ((slot - cum) << 8) | sym
-//   order-1: [256 B] raw context -> dense index (0xFF absent), then per dense
-//            context t: 4096 x u16 (sym << 8) | dense(sym), then 256 x u32
-//            (freq << 12) | cum.
+enum { kClsNone = 0, kClsO0 = 1, kClsO1Dense = 2, kClsO1Global = 3 };
+
+// Decode table arena per stream (bytes from tbl_off).
+//   order-0: 4096 x u32 packed ((freq - 1) << 20) | ((slot - cum) << 8) | sym.
+//   order-1 dense (|D| <= kDenseMax): D = present contexts and every symbol of
+//     their tables, in ascending byte order; DEAD = |D| marks "absent context".
+//     [0, (nd+1) * 4096)        chain table, u8: row d, column slot -> dense
+//                               symbol (rows of absent contexts and DEAD: DEAD)
+//     [.., + fc_bytes)          u32 (freq << 12) | cum, row = context, col = symbol
+//     [.., + 256)               dense index -> byte value
+//   order-1 global (more symbols): [256 B] raw context -> dense index (0xFF
+//     absent), then per present context t: 4096 x u16 (sym << 8) | dense(sym),
+//     then 256 x u32 (freq << 12) | cum.
+constexpr int kDenseMax = 47;
+__host__ __device__ inline uint32_t dense_fc_bytes(int nd) {
+    return (uint32_t)(((nd + 1) * (nd + 1) * 4 + 15) / 16 * 16);
+}
+__host__ __device__ inline uint32_t dense_table_bytes(int nd) {
+    return (uint32_t)((nd + 1) * 4096) + dense_fc_bytes(nd) + 256;
+}
 constexpr uint64_t kDecCtxMap = 0;
 constexpr uint64_t kDecO1Base = 256;
 constexpr uint64_t kDecO1Slot = 4096 * 2;
@@ -93,9 +112,19 @@ __host__ __device__ inline uint64_t dec_table_bytes(uint64_t src_len) {
     // A stream with K order-1 tables is at least 41 + 512 K bytes long.
     uint64_t k = src_len > 41 ? (src_len - 41) / 512 : 0;
     if (k > 256) k = 256;
-    uint64_t o1 = kDecO1Base + k * kDecO1Ctx;
-    return o1 > 16384 ? o1 : 16384;
+    uint64_t b = 16384;
+    if (k > 0) {
+        const uint64_t g = kDecO1Base + k * kDecO1Ctx;
+        const uint64_t d = dense_table_bytes(kDenseMax);
+        b = g > b ? g : b;
+        b = d > b ? d : b;
+    }
+    return b;
 }
+
+// Shared-memory layout of the decode kernels (one warp per CTA).
+constexpr uint32_t kRingBytes = 2048;       // renorm-word ring, 4 x 512 B segments
+constexpr uint32_t kOutRows = 3 * kDenseMax + 1;
 
 inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
@@ -110,8 +139,12 @@ void launch_enc_pack(EncBlock *blocks, int nblocks, const uint8_t *tbl, const ui
 
 void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint8_t *tbl,
                       int grid, cudaStream_t s);
-void launch_dec_run(const uint8_t *src, DecStream *streams, const uint32_t *order, int nstreams,
-                    const uint8_t *tbl, uint8_t *dst, int *queue, int grid, cudaStream_t s);
+// Runs the decode of the streams listed in `list` (all of class `cls`);
+// smem_bytes is the dynamic shared memory of the class (largest member).
+void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
+                    const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
+                    cudaStream_t s);
+uint32_t dec_smem_bytes(int cls, int nd);
 
 int sm_count(int device);
 

@@ -198,6 +198,7 @@ typedef struct fqxv_rans_stage_stat {
     char name[24];
     uint64_t launches;
     double ms;
+    uint64_t bytes;   /* algorithmic bytes (input read + output written) of those launches */
 } fqxv_rans_stage_stat;
 
 int fqxv_rans_ctx_set_profiling(fqxv_rans_ctx *ctx, int on);
