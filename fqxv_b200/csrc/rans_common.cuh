@@ -11,6 +11,14 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// Predicated stores: no branch, so unrolled rounds stay one basic block.
+__device__ __forceinline__ void st_u16_if(bool p, uint16_t *addr, uint32_t v) {
+    asm volatile(
+        "{\n .reg .pred q;\n setp.ne.b32 q, %0, 0;\n @q st.global.u16 [%1], %2;\n}" ::"r"((int)p), "l"(addr),
+        "h"((unsigned short)v)
+        : "memory");
+}
+
 __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
 #pragma unroll
     for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

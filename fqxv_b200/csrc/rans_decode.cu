@@ -181,8 +181,8 @@ __global__ void __launch_bounds__(kParseThreads)
                     const int dead = nd;
                     const int stride = nd + 1;
                     uint8_t *CT = T;
-                    uint32_t *FC = reinterpret_cast<uint32_t *>(T + (uint64_t)stride * 4096);
-                    uint8_t *DS = T + (uint64_t)stride * 4096 + dense_fc_bytes(nd);
+                    uint32_t *FC = reinterpret_cast<uint32_t *>(T + dense_chain_bytes(nd));
+                    uint8_t *DS = T + dense_chain_bytes(nd) + dense_fc_bytes(nd);
                     // Rows of dense indices without a table (and DEAD) map every
                     // slot to DEAD; the FC table starts zeroed.
                     for (int b = 0; b <= 256; b++) {
@@ -193,9 +193,9 @@ __global__ void __launch_bounds__(kParseThreads)
                         } else {
                             d = dead;
                         }
-                        uint32_t *row = reinterpret_cast<uint32_t *>(CT + (uint64_t)d * 4096);
+                        uint32_t *row = reinterpret_cast<uint32_t *>(CT + (uint64_t)d * kChainStride);
                         const uint32_t v = 0x01010101u * (uint32_t)dead;
-                        for (int i = tid; i < 1024; i += blockDim.x) row[i] = v;
+                        for (int i = tid; i < (int)kChainStride / 4; i += blockDim.x) row[i] = v;
                     }
                     for (int i = tid; i < stride * stride; i += blockDim.x) FC[i] = 0;
                     if (tid < 256 && dmap[tid] != 0xff) DS[dmap[tid]] = (uint8_t)tid;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kParseThreads)
                     for (int t = 0; t < K; t++) {
                         load_table(kHdr + kO1Bitmap + kO1Table * (uint64_t)t);
                         const int dc = dmap[ctxlist[t]];
-                        uint8_t *row = CT + (uint64_t)dc * 4096;
+                        uint8_t *row = CT + (uint64_t)dc * kChainStride;
                         for (int slot = tid; slot < (int)kTotFreq; slot += blockDim.x)
                             row[slot] = dmap[slot_sym((uint32_t)slot)];
                         if (tid < 256 && sfreq[tid])
@@ -365,8 +365,10 @@ struct WordRing {
             __syncwarp();
         }
     }
-    __device__ __forceinline__ uint32_t word(uint64_t j) const {
-        const uint64_t rel = lead + 2 * j;
+    // Word j of the region; only the low bits of j matter (the ring is a
+    // power-of-two window), so 32-bit arithmetic is exact here.
+    __device__ __forceinline__ uint32_t word(uint32_t j) const {
+        const uint32_t rel = lead + 2u * j;
         return (uint32_t)ring[rel & (kRingBytes - 1)] | ((uint32_t)ring[(rel + 1) & (kRingBytes - 1)] << 8);
     }
 };
@@ -377,12 +379,15 @@ struct WordRing {
 // than one word (only malformed streams do this); the round is then replayed
 // lane by lane from global memory. Returns false when the words run out
 // (scalar.rs:261, "truncated stream").
+// `first` is set for the first round only: a state read from the header may
+// be below 2^16, but every state a step produces is at least 2^16, after
+// which v = f (x >> 12) + offset >= 16 and one word always suffices.
 __device__ __forceinline__ bool renorm_round(uint32_t &v, bool need, const WordRing &R, uint64_t &wp,
-                                             uint64_t navail, uint32_t lt) {
+                                             uint64_t navail, uint32_t lt, bool first = true) {
     const int lane = threadIdx.x & 31;
-    const uint32_t cand = (wp + lane < navail) ? R.word(wp + lane) : 0u;
+    const uint32_t cand = (wp + lane < navail) ? R.word((uint32_t)(wp + lane)) : 0u;
     const uint32_t mask = __ballot_sync(0xffffffffu, need);
-    if (__any_sync(0xffffffffu, need && v == 0)) {
+    if (first && __any_sync(0xffffffffu, need && v == 0)) {
         uint64_t wpl = wp;
         bool ok = true;
         for (int l = 0; l < 32; l++) {
@@ -422,6 +427,28 @@ __device__ __forceinline__ int pop_job(int *queue) {
 // order-0 (scalar.rs:157-178, avx512.rs:78-134)
 // ---------------------------------------------------------------------------
 
+// One decode round through the general path: any lane may need several
+// words (states below 2^16 only come from a malformed header, so only the
+// first round can see them), lanes past n idle, and running out of words is
+// reported. Returns false on truncation.
+__device__ __forceinline__ bool o0_general_round(uint32_t &x, const uint32_t *__restrict__ P, uint64_t r,
+                                                 uint64_t n, WordRing &R, uint64_t &wp, uint64_t navail,
+                                                 uint8_t *__restrict__ out, uint32_t lt) {
+    const int lane = threadIdx.x & 31;
+    R.advance(wp);
+    const uint64_t i = r * 32 + lane;
+    const bool active = i < n;
+    const uint32_t e = P[x & (kTotFreq - 1)];
+    uint32_t v = ((e >> 20) + 1) * (x >> kScaleBits) + ((e >> 8) & 0xfffu);
+    const bool need = active && v < kRansL;
+    if (!renorm_round(v, need, R, wp, navail, lt)) return false;
+    if (active) {
+        out[i] = (uint8_t)e;
+        x = v;
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(32)
     dec_o0_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
@@ -451,22 +478,66 @@ __global__ void __launch_bounds__(32)
         uint8_t *out = dst + S.dst_off;
         uint64_t wp = 0;
         int status = FQXV_RANS_OK;
-        const uint64_t rounds = (n + 31) / 32;
-        for (uint64_t r = 0; r < rounds; r++) {
+        const uint64_t rounds = (n + 31) / 32, full = n / 32;
+        // Fast-path window: W0/W1 = words [wbase, wbase + 64) at lanes
+        // (lane, 32 + lane), PE0/PE1 = the table entries those words would
+        // select as the next slot, a = wp - wbase. A lane that renormalises
+        // takes word and next entry through one shuffle each, so the table
+        // lookup is off the round's critical path.
+        uint32_t W0 = 0, W1 = 0, PE0 = 0, PE1 = 0, a = 0, e = 0;
+        bool window = false;
+        uint64_t r = 0;
+        if (rounds && !o0_general_round(x, P, 0, n, R, wp, navail, out, lt)) status = FQXV_RANS_E_TRUNCATED;
+        r = 1;
+        constexpr int G = 8;  // rounds per branch-free group
+        while (status == FQXV_RANS_OK && r < rounds) {
+            // A group of G full rounds takes at most 32 G words and its window
+            // reads 64 ahead, so it cannot run out of words or ring.
+            if (r + G > full || wp + 32 * G + 64 > navail) {
+                if (!o0_general_round(x, P, r, n, R, wp, navail, out, lt)) status = FQXV_RANS_E_TRUNCATED;
+                r++;
+                window = false;
+                continue;
+            }
             R.advance(wp);
-            const uint64_t i = r * 32 + lane;
-            const bool active = i < n;
-            const uint32_t e = P[x & (kTotFreq - 1)];
-            uint32_t v = ((e >> 20) + 1) * (x >> kScaleBits) + ((e >> 8) & 0xfffu);
-            const bool need = active && v < kRansL;
-            if (!renorm_round(v, need, R, wp, navail, lt)) {
-                status = FQXV_RANS_E_TRUNCATED;
-                break;
+            uint32_t w32 = (uint32_t)wp;
+            if (!window) {
+                W0 = R.word(w32 + lane);
+                W1 = R.word(w32 + 32 + lane);
+                PE0 = P[W0 & (kTotFreq - 1)];
+                PE1 = P[W1 & (kTotFreq - 1)];
+                a = 0;
+                e = P[x & (kTotFreq - 1)];
+                window = true;
             }
-            if (active) {
-                out[i] = (uint8_t)e;
-                x = v;
+            uint8_t *op = out + r * 32 + lane;
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                const uint32_t nW0 = R.word(w32 + lane);
+                const uint32_t nW1 = R.word(w32 + 32 + lane);
+                const uint32_t nPE0 = P[nW0 & (kTotFreq - 1)];
+                const uint32_t nPE1 = P[nW1 & (kTotFreq - 1)];
+                const uint32_t v = ((e >> 20) + 1) * (x >> kScaleBits) + ((e >> 8) & 0xfffu);
+                const uint32_t ev = P[v & (kTotFreq - 1)];
+                const bool need = v < kRansL;
+                const uint32_t mask = __ballot_sync(0xffffffffu, need);
+                const uint32_t k = __popc(mask);
+                const uint32_t srcl = (a + __popc(mask & lt)) & 31u;
+                const bool lo = (uint32_t)lane >= a;
+                const uint32_t w = __shfl_sync(0xffffffffu, lo ? W0 : W1, srcl);
+                const uint32_t pe = __shfl_sync(0xffffffffu, lo ? PE0 : PE1, srcl);
+                op[32 * g] = (uint8_t)e;
+                x = need ? (v << 16) | w : v;
+                e = need ? pe : ev;
+                a = k;
+                w32 += k;
+                W0 = nW0;
+                W1 = nW1;
+                PE0 = nPE0;
+                PE1 = nPE1;
             }
+            wp += (uint32_t)(w32 - (uint32_t)wp);
+            r += G;
         }
         if (lane == 0) S.status = status;
         __syncwarp();
@@ -477,105 +548,125 @@ __global__ void __launch_bounds__(32)
 // order-1, dense tables in shared memory (scalar.rs:180-217)
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(32)
-    dec_o1d_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
-                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
-                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
-    extern __shared__ __align__(128) uint8_t sm[];
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ __align__(16) uint16_t s_slot[32];
-    __shared__ __align__(8) uint64_t s_out[kOutRows];
+// Decode one order-1 stream whose dense tables are in shared memory.
+//
+// Per round, the context chain d_i = chain[d_{i-1}][slot_i] of the 32 lanes
+// is resolved in four segments of eight: segment 0 from the known incoming
+// context, segments 1-3 for every possible incoming context (tasks
+// 1 + (k-1) nd + c), then three dependent lookups pick the real rows. TPL
+// (tasks per lane, ceil((1 + 3 nd) / 32)) is a template parameter and every
+// lane runs all TPL eight-step chains unconditionally, so they overlap.
+//
+// Rounds that cannot run out of words (and are not the first or the partial
+// last round) take a branch-free fast path: the ring advances by predication,
+// and a context without a table is only recorded, then reported once per
+// run of fast rounds -- such a stream fails anyway, and a truncation cannot
+// come earlier inside those rounds. Other rounds take the careful path with
+// every check of scalar.rs:202-215 in order.
+template <int TPL>
+__device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
+                                          uint32_t *__restrict__ s_slot, uint2 *__restrict__ s_out,
+                                          uint8_t *__restrict__ out, uint32_t lt) {
     const int lane = threadIdx.x;
-    const uint32_t lt = lanemask_lt();
-    TableStager st;
-    st.init(&bar);
-    for (;;) {
-        const int j = pop_job(queue);
-        if (j >= nlist) return;
-        DecStream &S = streams[list[j]];
-        const int nd = S.nd;
-        const uint32_t dead = (uint32_t)nd;
-        const uint32_t stride = (uint32_t)nd + 1;
-        st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
-        WordRing R;
-        R.init(src + S.words_off, S.words_len, sm + ring_off);
-        // Chain tasks of this lane: task 0 = segment 0 from the known context;
-        // task 1 + (k - 1) * nd + c = segment k (1..3) entered with context c.
-        const int ntask = 1 + 3 * nd;
-        int seg_q[5], c_q[5];
+    const int nd = S.nd;
+    const uint32_t dead = (uint32_t)nd;
+    const uint32_t stride = (uint32_t)nd + 1;
+    const int ntask = 1 + 3 * nd;
+    uint32_t seg_q[TPL], c_q[TPL], idx_q[TPL];
 #pragma unroll
-        for (int q = 0; q < 5; q++) {
-            const int t = lane + 32 * q;
-            seg_q[q] = t == 0 ? 0 : (t < ntask ? 1 + (t - 1) / nd : -1);
-            c_q[q] = t == 0 ? 0 : (t < ntask ? (t - 1) % nd : 0);
+    for (int q = 0; q < TPL; q++) {
+        const int t = lane + 32 * q;
+        const bool valid = t < ntask;
+        seg_q[q] = (!valid || t == 0) ? 0u : (uint32_t)(1 + (t - 1) / nd);
+        c_q[q] = (!valid || t == 0) ? 0u : (uint32_t)((t - 1) % nd);
+        idx_q[q] = !valid ? kOutRows : (t == 0 ? 0u : 1u + (seg_q[q] - 1) * (uint32_t)nd + c_q[q]);
+    }
+    const uint8_t *CT = sm;
+    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
+    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
+    const uint32_t deadw = 0x01010101u * dead;
+    const uint32_t cmax = nd > 0 ? (uint32_t)nd - 1 : 0u;
+    const uint64_t n = S.n;
+    const uint64_t navail = S.words_len / 2;
+    uint32_t x = S.states[lane];
+    uint64_t wp = 0;
+    uint32_t din = (uint32_t)S.start;
+    const uint64_t rounds = (n + 31) / 32, full = n / 32;
+    const int seg = lane >> 3, pos = lane & 7;
+
+    // Chain rows of this round for every task, then the resolved symbol d and
+    // context ctx of this lane. Row bytes: d_0 is the top byte of .x, d_7 the
+    // low byte of .y.
+    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
+        s_slot[lane] = slot;
+        __syncwarp();
+        uint2 rows[TPL];
+#pragma unroll
+        for (int q = 0; q < TPL; q++) {
+            const uint4 sa = *reinterpret_cast<const uint4 *>(s_slot + 8 * seg_q[q]);
+            const uint4 sb = *reinterpret_cast<const uint4 *>(s_slot + 8 * seg_q[q] + 4);
+            const uint32_t sl[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
+            uint32_t dd = (q == 0 && lane == 0) ? din : c_q[q];
+            uint32_t hi = 0, lo = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                dd = CT[dd * kChainStride + sl[k]];
+                hi = hi * 256u + dd;
+            }
+#pragma unroll
+            for (int k = 4; k < 8; k++) {
+                dd = CT[dd * kChainStride + sl[k]];
+                lo = lo * 256u + dd;
+            }
+            rows[q] = make_uint2(hi, lo);
         }
-        if (!st.wait()) {
-            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
-            st.wait();
-            return;
-        }
-        const uint8_t *CT = sm;
-        const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + stride * 4096);
-        const uint8_t *DS = sm + stride * 4096 + dense_fc_bytes(nd);
-        const uint64_t deadrow = 0x0101010101010101ull * dead;
-        const uint64_t n = S.n;
-        const uint64_t navail = S.words_len / 2;
-        uint32_t x = S.states[lane];
-        uint8_t *out = dst + S.dst_off;
-        uint64_t wp = 0;
-        uint32_t din = (uint32_t)S.start;
-        int status = FQXV_RANS_OK;
-        const uint64_t rounds = (n + 31) / 32;
-        const int seg = lane >> 3, pos = lane & 7;
-        for (uint64_t r = 0; r < rounds; r++) {
+#pragma unroll
+        for (int q = 0; q < TPL; q++) s_out[idx_q[q]] = rows[q];
+        __syncwarp();
+        const uint2 r0 = s_out[0];
+        const uint32_t c1 = r0.y & 0xffu;
+        uint2 r1 = s_out[1 + (c1 < cmax ? c1 : cmax)];
+        if (c1 == dead) r1 = make_uint2(deadw, deadw);
+        const uint32_t c2 = r1.y & 0xffu;
+        uint2 r2 = s_out[1 + nd + (c2 < cmax ? c2 : cmax)];
+        if (c2 == dead) r2 = make_uint2(deadw, deadw);
+        const uint32_t c3 = r2.y & 0xffu;
+        uint2 r3 = s_out[1 + 2 * nd + (c3 < cmax ? c3 : cmax)];
+        if (c3 == dead) r3 = make_uint2(deadw, deadw);
+        const uint2 row = seg == 0 ? r0 : seg == 1 ? r1 : seg == 2 ? r2 : r3;
+        const uint32_t in = seg == 0 ? din : seg == 1 ? c1 : seg == 2 ? c2 : c3;
+        const uint32_t pw = pos < 4 ? row.x : row.y;
+        const uint32_t sh = 24u - 8u * (uint32_t)(pos & 3);
+        d = (pw >> sh) & 0xffu;
+        const uint32_t pm = pos <= 4 ? row.x : row.y;  // byte pos - 1
+        const uint32_t shm = 24u - 8u * (uint32_t)((pos + 3) & 3);
+        ctx = pos == 0 ? in : (pm >> shm) & 0xffu;
+        din = r3.y & 0xffu;
+        __syncwarp();
+    };
+
+    uint64_t r = 0;
+    int status = FQXV_RANS_OK;
+    while (r < rounds && status == FQXV_RANS_OK) {
+        const int64_t spare = (int64_t)navail - (int64_t)wp - 64;
+        int64_t cnt = spare > 0 ? spare / 32 : 0;
+        const int64_t left_full = r < full ? (int64_t)(full - r) : 0;
+        if (cnt > left_full) cnt = left_full;
+        if (r == 0 || cnt <= 0) {
+            // careful round (scalar.rs:202-215 in order)
             R.advance(wp);
             const uint64_t i = r * 32 + lane;
             const bool active = i < n;
             const uint32_t slot = x & (kTotFreq - 1);
-            s_slot[lane] = (uint16_t)slot;
-            __syncwarp();
-#pragma unroll
-            for (int q = 0; q < 5; q++) {
-                if (seg_q[q] >= 0) {
-                    const uint4 sv = *reinterpret_cast<const uint4 *>(s_slot + 8 * seg_q[q]);
-                    const uint32_t sl[8] = {sv.x & 0xffffu, sv.x >> 16, sv.y & 0xffffu, sv.y >> 16,
-                                            sv.z & 0xffffu, sv.z >> 16, sv.w & 0xffffu, sv.w >> 16};
-                    uint32_t d = (lane == 0 && q == 0) ? din : (uint32_t)c_q[q];
-                    uint64_t row = 0;
-#pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        d = CT[(d << 12) | sl[k]];
-                        row |= (uint64_t)d << (8 * k);
-                    }
-                    const int idx = (lane == 0 && q == 0) ? 0 : 1 + (seg_q[q] - 1) * nd + c_q[q];
-                    s_out[idx] = row;
-                }
-            }
-            __syncwarp();
-            const uint64_t r0 = s_out[0];
-            const uint32_t c1 = (uint32_t)(r0 >> 56);
-            const uint64_t r1 = c1 == dead ? deadrow : s_out[1 + c1];
-            const uint32_t c2 = (uint32_t)(r1 >> 56);
-            const uint64_t r2 = c2 == dead ? deadrow : s_out[1 + nd + c2];
-            const uint32_t c3 = (uint32_t)(r2 >> 56);
-            const uint64_t r3 = c3 == dead ? deadrow : s_out[1 + 2 * nd + c3];
-            const uint64_t row = seg == 0 ? r0 : seg == 1 ? r1 : seg == 2 ? r2 : r3;
-            const uint32_t in = seg == 0 ? din : seg == 1 ? c1 : seg == 2 ? c2 : c3;
-            const uint32_t d = (uint32_t)(row >> (8 * pos)) & 0xffu;
-            const uint32_t ctx = pos == 0 ? in : (uint32_t)(row >> (8 * pos - 8)) & 0xffu;
-            din = (uint32_t)(r3 >> 56);
-            __syncwarp();
-            // A lane whose context has no table reads DEAD (scalar.rs:204-206).
+            uint32_t d, ctx;
+            resolve(slot, d, ctx);
             const uint32_t deadmask = __ballot_sync(0xffffffffu, active && d == dead);
             const int absent_at = deadmask ? __ffs(deadmask) - 1 : 32;
             const bool valid = active && lane < absent_at;
-            uint32_t v = 0;
-            if (valid) {
-                const uint32_t fc = FC[ctx * stride + d];
-                v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
-            }
+            const uint32_t fc = FC[ctx * stride + d];
+            uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
             const bool need = valid && v < kRansL;
-            if (!renorm_round(v, need, R, wp, navail, lt)) {
+            if (!renorm_round(v, need, R, wp, navail, lt, r == 0)) {
                 status = FQXV_RANS_E_TRUNCATED;
                 break;
             }
@@ -587,6 +678,80 @@ __global__ void __launch_bounds__(32)
                 out[i] = DS[d];
                 x = v;
             }
+            r++;
+            continue;
+        }
+        // fast rounds: each takes at most 32 words, cnt of them fit.
+        R.advance(wp);
+        uint32_t w32 = (uint32_t)wp;
+        uint32_t adv_at = (uint32_t)((512u * (uint32_t)(R.next_seg - 3) - R.lead + 1u) / 2u);
+        uint32_t sawdead = 0;
+        uint8_t *op = out + r * 32 + lane;
+        for (int64_t c = 0; c < cnt; c++) {
+            // predicated one-segment ring advance (a round moves <= 64 bytes)
+            const bool adv = w32 - (uint32_t)wp >= adv_at - (uint32_t)wp;
+            if (adv) {
+                R.put(R.next_seg, R.pend);
+                R.next_seg++;
+                R.pend = R.fetch(R.next_seg);
+                adv_at += 256u;
+            }
+            __syncwarp();
+            const uint32_t cand = R.word(w32 + lane);
+            const uint32_t slot = x & (kTotFreq - 1);
+            uint32_t d, ctx;
+            resolve(slot, d, ctx);
+            sawdead |= d == dead;
+            const uint32_t fc = FC[ctx * stride + d];
+            const uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
+            const bool need = v < kRansL;
+            const uint32_t mask = __ballot_sync(0xffffffffu, need);
+            const uint32_t w = __shfl_sync(0xffffffffu, cand, __popc(mask & lt) & 31);
+            *op = DS[d];
+            op += 32;
+            x = need ? (v << 16) | w : v;
+            w32 += __popc(mask);
+        }
+        wp += (uint32_t)(w32 - (uint32_t)wp);
+        r += (uint64_t)cnt;
+        if (__any_sync(0xffffffffu, sawdead != 0)) status = FQXV_RANS_E_ABSENT_CONTEXT;
+    }
+    return status;
+}
+
+__global__ void __launch_bounds__(32)
+    dec_o1d_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
+                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
+                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(16) uint32_t s_slot[32];
+    __shared__ __align__(16) uint2 s_out[kOutRows + 1];
+    const int lane = threadIdx.x;
+    const uint32_t lt = lanemask_lt();
+    TableStager st;
+    st.init(&bar);
+    for (;;) {
+        const int j = pop_job(queue);
+        if (j >= nlist) return;
+        DecStream &S = streams[list[j]];
+        st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
+        WordRing R;
+        R.init(src + S.words_off, S.words_len, sm + ring_off);
+        if (!st.wait()) {
+            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
+            st.wait();
+            return;
+        }
+        uint8_t *out = dst + S.dst_off;
+        const int tpl = (1 + 3 * S.nd + 31) / 32;
+        int status;
+        switch (tpl) {
+            case 1: status = o1d_stream<1>(S, sm, R, s_slot, s_out, out, lt); break;
+            case 2: status = o1d_stream<2>(S, sm, R, s_slot, s_out, out, lt); break;
+            case 3: status = o1d_stream<3>(S, sm, R, s_slot, s_out, out, lt); break;
+            case 4: status = o1d_stream<4>(S, sm, R, s_slot, s_out, out, lt); break;
+            default: status = o1d_stream<5>(S, sm, R, s_slot, s_out, out, lt); break;
         }
         if (lane == 0) S.status = status;
         __syncwarp();

@@ -176,74 +176,123 @@ __global__ void __launch_bounds__(kModelThreads)
     }
 }
 
-// Reverse-order encode of one block by one warp (scalar.rs:39-43 / :84-90,
-// the state map of model.rs:125-133 computed as avx2.rs:383-393). Lane l owns
-// state l; round r covers positions [32r, 32r + 32). Rounds run from the last
-// to the first; the renorm words of a round are emitted high lane first, so
-// they are stored back to front at [wend - k, wend) in ascending lane order
+// One encode step of a lane (scalar.rs:120-127 with the map of
+// model.rs:125-133, computed as avx2.rs:383-393): a state at or above
+// x_max = f << 20 gives up its low 16 bits (at most one word), then
+// x' = v + cum + q (4096 - f) with q = v / f from the magic reciprocal and one
+// correction. Both quotient candidates (with and without the renorm shift)
+// start at once, so the chain is compare -> select -> multiply -> compare ->
+// select. Returns whether the lane emits a word (its pre-step low 16 bits).
+__device__ __forceinline__ bool enc_step(uint32_t &x, uint2 e, bool active) {
+    const uint32_t f = e.y >> kScaleBits;
+    const uint32_t cum = e.y & (kTotFreq - 1);
+    const uint32_t xmax_m1 = (f << 20) - 1u;  // wraps to 2^32 - 1 for f == 4096: never emits
+    const uint32_t cmpl = kTotFreq - f;
+    const bool need = active && x > xmax_m1;
+    const uint32_t xs = x >> 16;
+    const uint32_t qa = __umulhi(x, e.x);
+    const uint32_t qb = __umulhi(xs, e.x);
+    const uint32_t v = need ? xs : x;
+    const uint32_t q0 = need ? qb : qa;
+    const uint32_t r0 = v - q0 * f;
+    const uint32_t x0 = v + cum + q0 * cmpl;
+    const uint32_t xn = r0 >= f ? x0 + cmpl : x0;
+    if (active) x = xn;
+    return need;
+}
+
+// Emit the words of one round: the reference emits them high lane first
+// (scalar.rs:39-43), so stored below `wptr` they land in ascending lane order
 // and the finished region is already in decode order (scalar.rs:134-139).
+__device__ __forceinline__ void enc_emit(bool need, uint32_t word, uint16_t *__restrict__ &wptr, uint32_t lt) {
+    const uint32_t mask = __ballot_sync(0xffffffffu, need);
+    wptr -= __popc(mask);
+    st_u16_if(need, wptr + __popc(mask & lt), word);
+}
+
+// Reverse-order encode of one block by one warp (scalar.rs:39-43 / :84-90).
+// Lane l owns state l; round r covers positions [32r, 32r + 32). The partial
+// top round goes first, then the full rounds from the last to the first in
+// chunks of 16 whose symbols are loaded one chunk ahead. Word emission (a
+// warp vote per round) is kept off the state chain: a chunk records its
+// emit flags and pre-step states, and its words are written while the next
+// chunk's states are computed.
 template <int ORDER>
 __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint64_t n,
                                             const uint2 *__restrict__ tab,
-                                            const uint8_t *__restrict__ umap, int nu,
+                                            const uint8_t *__restrict__ umap, uint32_t nu,
                                             uint16_t *__restrict__ words, uint64_t word_end,
                                             uint64_t &nwords, uint32_t &state) {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = lanemask_lt();
     uint32_t x = kRansL;
-    uint64_t wend = word_end;
-    const int64_t R = (int64_t)((n + 31) / 32);
-    uint32_t cur[16], nxt[16];
+    uint16_t *wptr = words + word_end;
+    const int64_t full = (int64_t)(n / 32);
+    const uint32_t rem = (uint32_t)(n % 32);
+    // Table entry of symbol s with predecessor `prev` (order-1: scalar.rs:85).
+    auto entry = [&](uint32_t s, uint32_t prev) -> uint2 {
+        if (ORDER == 0) return tab[s];
+        return __ldg(tab + (uint32_t)umap[prev] * nu + umap[s]);
+    };
+    if (rem) {
+        const uint64_t i = (uint64_t)full * 32 + lane;
+        const bool active = lane < (int)rem;
+        const uint32_t s = active ? (uint32_t)__ldg(p + i) : 0u;
+        uint32_t prev = 0;
+        if (ORDER == 1) prev = (active && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
+        const uint2 e = active ? entry(s, prev) : make_uint2(0u, 0u);
+        const uint32_t x_before = x;
+        const bool need = enc_step(x, e, active);
+        enc_emit(need, x_before, wptr, lt);
+    }
+    uint32_t cur[16], nxt[16], wv[16], pwv[16];
+    uint32_t pbits = 0;  // emit flags of the previous chunk (bit k = round rt + 16 - k)
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        const int64_t r = R - 1 - k;
-        const uint64_t i = (uint64_t)r * 32 + lane;
-        cur[k] = (r >= 0 && i < n) ? (uint32_t)__ldg(p + i) : 0u;
+        const int64_t r = full - 1 - k;
+        cur[k] = r >= 0 ? (uint32_t)__ldg(p + (uint64_t)r * 32 + lane) : 0u;
+        pwv[k] = 0;
     }
-    for (int64_t rtop = R - 1; rtop >= 0; rtop -= 16) {
+    for (int64_t rt = full - 1; rt >= 0; rt -= 16) {
+        if (rt >= 31) {
+            const uint8_t *pc = p + (uint64_t)(rt - 16) * 32 + lane;
+#pragma unroll
+            for (int k = 0; k < 16; k++) nxt[k] = (uint32_t)__ldg(pc - 32 * k);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int64_t r = rt - 16 - k;
+                nxt[k] = r >= 0 ? (uint32_t)__ldg(p + (uint64_t)r * 32 + lane) : 0u;
+            }
+        }
+        const bool whole = rt >= 15;
+        uint32_t bits = 0;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
-            const int64_t r = rtop - 16 - k;
-            const uint64_t i = (uint64_t)r * 32 + lane;
-            nxt[k] = (r >= 0 && i < n) ? (uint32_t)__ldg(p + i) : 0u;
+            uint32_t prev = 0;
+            if (ORDER == 1) {
+                // lane l > 0: lane l-1 of this round; lane 0: lane 31 of the
+                // round below (a guarded load gives 0 below round 0, which is
+                // the reference's initial context).
+                const uint32_t up = __shfl_up_sync(0xffffffffu, cur[k], 1);
+                const uint32_t p31 = __shfl_sync(0xffffffffu, k < 15 ? cur[k < 15 ? k + 1 : 15] : nxt[0], 31);
+                prev = lane ? up : p31;
+            }
+            wv[k] = x;
+            const bool active = whole || k <= rt;
+            if (enc_step(x, entry(cur[k], prev), active)) bits |= 1u << k;
+            enc_emit((pbits >> k) & 1u, pwv[k], wptr, lt);
         }
+        pbits = bits;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
-            const int64_t r = rtop - k;
-            if (r < 0) break;
-            const uint64_t i = (uint64_t)r * 32 + lane;
-            const bool active = i < n;
-            const uint32_t s = cur[k];
-            uint2 e;
-            if (ORDER == 0) {
-                e = tab[s];
-            } else {
-                const uint32_t up = __shfl_up_sync(0xffffffffu, s, 1);
-                const uint32_t p31 = __shfl_sync(0xffffffffu, k < 15 ? cur[k + 1 < 16 ? k + 1 : 15] : nxt[0], 31);
-                const uint32_t prev = lane ? up : (r == 0 ? 0u : p31);
-                e = __ldg(tab + (uint32_t)umap[prev] * (uint32_t)nu + umap[s]);
-            }
-            const uint32_t f = e.y >> kScaleBits;
-            const uint32_t cum = e.y & (kTotFreq - 1);
-            // scalar.rs:122: emit while x >= x_max = f << 20 (at most once).
-            const bool need = active && (x >> 20) >= f;
-            const uint32_t mask = __ballot_sync(0xffffffffu, need);
-            const uint32_t kw = __popc(mask);
-            if (need) words[wend - kw + __popc(mask & lt)] = (uint16_t)(x & 0xffffu);
-            wend -= kw;
-            const uint32_t v = need ? x >> 16 : x;
-            uint32_t q = __umulhi(v, e.x);
-            uint32_t rem = v - q * f;
-            if (rem >= f) {
-                q += 1;
-                rem -= f;
-            }
-            if (active) x = (q << kScaleBits) + rem + cum;
+            cur[k] = nxt[k];
+            pwv[k] = wv[k];
         }
-#pragma unroll
-        for (int k = 0; k < 16; k++) cur[k] = nxt[k];
     }
-    nwords = word_end - wend;
+#pragma unroll
+    for (int k = 0; k < 16; k++) enc_emit((pbits >> k) & 1u, pwv[k], wptr, lt);
+    nwords = (uint64_t)((words + word_end) - wptr);
     state = x;
 }
 
@@ -278,8 +327,8 @@ __global__ void __launch_bounds__(kEncWarpsPerCta * 32)
 #pragma unroll
                 for (int k = 0; k < 8; k++) s_umap[warp][lane * 8 + k] = T[kTblUmap + lane * 8 + k];
                 __syncwarp();
-                encode_warp<1>(p, n, reinterpret_cast<const uint2 *>(T + kTblO1), s_umap[warp], B.nu,
-                               words, word_end, nw, st);
+                encode_warp<1>(p, n, reinterpret_cast<const uint2 *>(T + kTblO1), s_umap[warp],
+                               (uint32_t)B.nu, words, word_end, nw, st);
             }
         }
         B.states[job.order][lane] = st;

@@ -89,7 +89,7 @@ enum { kClsNone = 0, kClsO0 = 1, kClsO1Dense = 2, kClsO1Global = 3 };
 //   order-0: 4096 x u32 packed ((freq - 1) << 20) | ((slot - cum) << 8) | sym.
 //   order-1 dense (|D| <= kDenseMax): D = present contexts and every symbol of
 //     their tables, in ascending byte order; DEAD = |D| marks "absent context".
-//     [0, (nd+1) * 4096)        chain table, u8: row d, column slot -> dense
+//     [0, chain_bytes)          chain table, u8: row d (stride 4100), slot -> dense
 //                               symbol (rows of absent contexts and DEAD: DEAD)
 //     [.., + fc_bytes)          u32 (freq << 12) | cum, row = context, col = symbol
 //     [.., + 256)               dense index -> byte value
@@ -97,11 +97,17 @@ enum { kClsNone = 0, kClsO0 = 1, kClsO1Dense = 2, kClsO1Global = 3 };
 //     absent), then per present context t: 4096 x u16 (sym << 8) | dense(sym),
 //     then 256 x u32 (freq << 12) | cum.
 constexpr int kDenseMax = 47;
+// Chain rows are 4100 bytes apart, not 4096: lanes that follow different
+// candidate contexts through the same slot then hit different banks.
+constexpr uint32_t kChainStride = 4100;
+__host__ __device__ inline uint32_t dense_chain_bytes(int nd) {
+    return (uint32_t)(((nd + 1) * kChainStride + 15) / 16 * 16);
+}
 __host__ __device__ inline uint32_t dense_fc_bytes(int nd) {
     return (uint32_t)(((nd + 1) * (nd + 1) * 4 + 15) / 16 * 16);
 }
 __host__ __device__ inline uint32_t dense_table_bytes(int nd) {
-    return (uint32_t)((nd + 1) * 4096) + dense_fc_bytes(nd) + 256;
+    return dense_chain_bytes(nd) + dense_fc_bytes(nd) + 256;
 }
 constexpr uint64_t kDecCtxMap = 0;
 constexpr uint64_t kDecO1Base = 256;
