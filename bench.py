@@ -51,11 +51,12 @@ def build_workload(name: str, seed: int):
     if name == "config0":
         data, spans = W.config0(seed=seed)
         return data, spans, 0, "1 x 1 MiB binned quality block, order-0", {}
+    workers = min(32, os.cpu_count() or 1)
     if name == "config2":
-        data, spans, kinds = W.config2(seed=seed)
+        data, spans, kinds = W.config2(seed=seed, workers=workers)
         return data, spans, 2, "4096 mixed blocks 4 KiB-4 MiB, both orders, keep the smaller", {}
     if name == "config3":
-        d2, s2, _ = W.config2(seed=seed)
+        d2, s2, _ = W.config2(seed=seed, workers=workers)
         d3, s3 = W.config3_ont(seed=seed)
         s3 = s3.copy()
         s3[:, 0] += len(d2)
@@ -194,13 +195,140 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args, rank: int) -> None:
+    """config4: requests arrive as a Poisson process at offered loads (fractions
+    of the measured batched capacity); 70% decompress / 30% compress; sizes
+    log-uniform 16 KiB - 64 MiB; stream types of configs 2 and 3. The server
+    admits by device memory under a 40 GB cap and batches continuously; the
+    same schedule is also run through plain per-request calls."""
+    if rank != 0:
+        return
+    import queue as _queue
+    import random
+
+    import torch
+
+    from fqxv_b200 import rans
+    from fqxv_b200.serve import Server
+    from oracle import oracle
+
+    rng = np.random.default_rng(args.seed)
+    kinds = ["binned", "full", "acgt", "names", "ont"]
+    nreq = args.requests
+    reqs = []
+    for i in range(nreq):
+        size = int(np.exp(rng.uniform(np.log(16 << 10), np.log(64 << 20))))
+        kind = kinds[int(rng.integers(0, len(kinds)))]
+        if kind == "ont":
+            data = W.ont_reads(max(1, size // 8000 + 1), args.seed + i)[:size]
+        else:
+            data = W.GENERATORS[kind](size, args.seed + i)
+        raw = data.tobytes()
+        if rng.random() < 0.7:
+            e0, e1 = oracle.encode(raw, 0), oracle.encode(raw, 1)
+            reqs.append(("dec", e1 if len(e1) < len(e0) else e0, len(raw)))
+        else:
+            reqs.append(("enc", raw, len(raw)))
+    total = sum(r[2] for r in reqs)
+    torch.cuda.init()
+    expect = [None] * nreq
+
+    def run_server(arrivals):
+        lat = [0.0] * nreq
+        with Server(device=0, workers=args.workers, hbm_cap=40 << 30) as srv:
+            ids = [None] * nreq
+            t0 = time.perf_counter()
+            for i, (k, d, n) in enumerate(reqs):
+                wait = arrivals[i] - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                ids[i] = srv.submit_decode(d) if k == "dec" else srv.submit_encode(d, rans.Order.BestTie0)
+            outs = []
+            for i in range(nreq):
+                outs.append(srv.result(ids[i]))
+                lat[i] = srv.last_latency_us / 1e3
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+        return outs, lat, wall, st
+
+    def run_plain(arrivals):
+        # one request at a time through the single-call C ABI, in arrival order
+        lat = [0.0] * nreq
+        q = _queue.Queue()
+        done = [None] * nreq
+        outs = [None] * nreq
+
+        def worker():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                i, t_arr = item
+                k, d, n = reqs[i]
+                outs[i] = rans.decode(d) if k == "dec" else rans.encode(d, rans.Order.BestTie0)
+                done[i] = time.perf_counter()
+        th = threading.Thread(target=worker)
+        th.start()
+        t0 = time.perf_counter()
+        arr_abs = [0.0] * nreq
+        for i in range(nreq):
+            wait = arrivals[i] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            arr_abs[i] = time.perf_counter()
+            q.put((i, arr_abs[i]))
+        q.put(None)
+        th.join()
+        wall = time.perf_counter() - t0
+        for i in range(nreq):
+            lat[i] = (done[i] - arr_abs[i]) * 1e3
+        return outs, lat, wall
+
+    # capacity: everything submitted at once
+    outs, lat, wall, st = run_server([0.0] * nreq)
+    for i, (k, d, n) in enumerate(reqs):
+        expect[i] = outs[i]
+    cap_gbs = total / wall / 1e9
+    levels = []
+    for load in args.loads:
+        lam = load * cap_gbs * 1e9 / (total / nreq)  # requests per second
+        arrivals = list(np.cumsum(np.random.default_rng(args.seed + int(load * 100)).exponential(1.0 / lam, nreq)))
+        outs, lat, wall, st = run_server(arrivals)
+        same = all(o == e for o, e in zip(outs, expect))
+        outs_p, lat_p, wall_p = run_plain(arrivals)
+        same_p = all(o == e for o, e in zip(outs_p, expect))
+        levels.append({
+            "offered_load": load, "offered_gbs": round(load * cap_gbs, 3),
+            "served": {"gbs": round(total / wall / 1e9, 3), "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                       "p99_ms": round(float(np.percentile(lat, 99)), 2), "batches": st["batches"],
+                       "byte_identical": bool(same)},
+            "plain_per_request": {"gbs": round(total / wall_p / 1e9, 3),
+                                  "p50_ms": round(float(np.percentile(lat_p, 50)), 2),
+                                  "p99_ms": round(float(np.percentile(lat_p, 99)), 2),
+                                  "byte_identical": bool(same_p)},
+        })
+    line = {
+        "metric": "rANS Nx16 serving: p50/p99 latency vs offered load (GB/s of uncompressed bytes)",
+        "value": levels[-1]["served"]["gbs"], "unit": "GB/s", "n_gpus": 1, "steps": len(args.loads),
+        "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "config4", "requests": nreq, "bytes": total, "decompress_fraction": 0.7,
+                   "sizes": "log-uniform 16 KiB - 64 MiB", "hbm_cap_bytes": 40 << 30, "workers": args.workers},
+        "capacity_gbs": round(cap_gbs, 3), "levels": levels,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config1", choices=["config1", "config0", "config2", "config3"])
+    ap.add_argument("--workload", default="config1", choices=["config1", "config0", "config2", "config3", "config4"])
+    ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
+    ap.add_argument("--workers", type=int, default=4, help="config4: server workers (streams)")
+    ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -214,6 +342,9 @@ def main() -> None:
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "config4":
+        run_serving(args, rank)
         return
 
     import torch

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libfqxv_rans_gpu.so")
-SOURCES = ["rans_encode.cu", "rans_decode.cu", "rans_capi.cu", "rans_noalloc.cu"]
+SOURCES = ["rans_encode.cu", "rans_decode.cu", "rans_capi.cu", "rans_noalloc.cu", "rans_server.cu"]
 HEADERS = ["rans_internal.cuh", "rans_common.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

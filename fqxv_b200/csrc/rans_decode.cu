@@ -548,14 +548,17 @@ __global__ void __launch_bounds__(32)
 // order-1, dense tables in shared memory (scalar.rs:180-217)
 // ---------------------------------------------------------------------------
 
-// Decode one order-1 stream whose dense tables are in shared memory.
+// Decode one order-1 stream whose dense tables are in shared memory, with
+// four warps (kO1Warps) per stream.
 //
 // Per round, the context chain d_i = chain[d_{i-1}][slot_i] of the 32 lanes
 // is resolved in four segments of eight: segment 0 from the known incoming
 // context, segments 1-3 for every possible incoming context (tasks
-// 1 + (k-1) nd + c), then three dependent lookups pick the real rows. TPL
-// (tasks per lane, ceil((1 + 3 nd) / 32)) is a template parameter and every
-// lane runs all TPL eight-step chains unconditionally, so they overlap.
+// 1 + (k-1) nd + c), then three dependent lookups pick the real rows. The
+// 1 + 3 nd eight-step chains are spread over all 128 threads (TPL per thread,
+// a template parameter), so the stream's SM runs them on all four schedulers.
+// Warp 0 owns the 32 states, the renorm words and the output; the other warps
+// only run chains. Two named barriers per round: slots ready, rows ready.
 //
 // Rounds that cannot run out of words (and are not the first or the partial
 // last round) take a branch-free fast path: the ring advances by predication,
@@ -563,50 +566,47 @@ __global__ void __launch_bounds__(32)
 // run of fast rounds -- such a stream fails anyway, and a truncation cannot
 // come earlier inside those rounds. Other rounds take the careful path with
 // every check of scalar.rs:202-215 in order.
+constexpr int kO1Warps = 4;
+constexpr int kO1Threads = 32 * kO1Warps;
+
+__device__ __forceinline__ void named_bar(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kO1Threads) : "memory");
+}
+
+struct O1Shared {
+    uint32_t slot[32];
+    uint2 out[kOutRows + 1];
+    uint32_t din;
+    int go;
+};
+
 template <int TPL>
 __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
-                                          uint32_t *__restrict__ s_slot, uint2 *__restrict__ s_out,
-                                          uint8_t *__restrict__ out, uint32_t lt) {
-    const int lane = threadIdx.x;
+                                          O1Shared &sh, uint8_t *__restrict__ out, uint32_t lt) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nd = S.nd;
     const uint32_t dead = (uint32_t)nd;
-    const uint32_t stride = (uint32_t)nd + 1;
     const int ntask = 1 + 3 * nd;
     uint32_t seg_q[TPL], c_q[TPL], idx_q[TPL];
 #pragma unroll
     for (int q = 0; q < TPL; q++) {
-        const int t = lane + 32 * q;
+        const int t = tid + kO1Threads * q;
         const bool valid = t < ntask;
         seg_q[q] = (!valid || t == 0) ? 0u : (uint32_t)(1 + (t - 1) / nd);
         c_q[q] = (!valid || t == 0) ? 0u : (uint32_t)((t - 1) % nd);
         idx_q[q] = !valid ? kOutRows : (t == 0 ? 0u : 1u + (seg_q[q] - 1) * (uint32_t)nd + c_q[q]);
     }
     const uint8_t *CT = sm;
-    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
-    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
-    const uint32_t deadw = 0x01010101u * dead;
-    const uint32_t cmax = nd > 0 ? (uint32_t)nd - 1 : 0u;
-    const uint64_t n = S.n;
-    const uint64_t navail = S.words_len / 2;
-    uint32_t x = S.states[lane];
-    uint64_t wp = 0;
-    uint32_t din = (uint32_t)S.start;
-    const uint64_t rounds = (n + 31) / 32, full = n / 32;
-    const int seg = lane >> 3, pos = lane & 7;
-
-    // Chain rows of this round for every task, then the resolved symbol d and
-    // context ctx of this lane. Row bytes: d_0 is the top byte of .x, d_7 the
-    // low byte of .y.
-    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
-        s_slot[lane] = slot;
-        __syncwarp();
+    // Chain rows of this round for this thread's tasks. Row bytes: d_0 is the
+    // top byte of .x, d_7 the low byte of .y.
+    auto tasks = [&](uint32_t din) {
         uint2 rows[TPL];
 #pragma unroll
         for (int q = 0; q < TPL; q++) {
-            const uint4 sa = *reinterpret_cast<const uint4 *>(s_slot + 8 * seg_q[q]);
-            const uint4 sb = *reinterpret_cast<const uint4 *>(s_slot + 8 * seg_q[q] + 4);
+            const uint4 sa = *reinterpret_cast<const uint4 *>(sh.slot + 8 * seg_q[q]);
+            const uint4 sb = *reinterpret_cast<const uint4 *>(sh.slot + 8 * seg_q[q] + 4);
             const uint32_t sl[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
-            uint32_t dd = (q == 0 && lane == 0) ? din : c_q[q];
+            uint32_t dd = (q == 0 && tid == 0) ? din : c_q[q];
             uint32_t hi = 0, lo = 0;
 #pragma unroll
             for (int k = 0; k < 4; k++) {
@@ -621,23 +621,56 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
             rows[q] = make_uint2(hi, lo);
         }
 #pragma unroll
-        for (int q = 0; q < TPL; q++) s_out[idx_q[q]] = rows[q];
-        __syncwarp();
-        const uint2 r0 = s_out[0];
+        for (int q = 0; q < TPL; q++) sh.out[idx_q[q]] = rows[q];
+    };
+
+    if (warp != 0) {
+        // helper warps: run this thread's chains every round until told to stop
+        for (;;) {
+            named_bar(1);
+            if (!sh.go) break;
+            tasks(0);
+            named_bar(2);
+        }
+        return FQXV_RANS_OK;
+    }
+
+    const uint32_t stride = (uint32_t)nd + 1;
+    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
+    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
+    const uint32_t deadw = 0x01010101u * dead;
+    const uint32_t cmax = nd > 0 ? (uint32_t)nd - 1 : 0u;
+    const uint64_t n = S.n;
+    const uint64_t navail = S.words_len / 2;
+    uint32_t x = S.states[lane];
+    uint64_t wp = 0;
+    uint32_t din = (uint32_t)S.start;
+    const uint64_t rounds = (n + 31) / 32, full = n / 32;
+    const int seg = lane >> 3, pos = lane & 7;
+
+    // One round of chains across the CTA, then the resolved symbol d and
+    // context ctx of this lane (warp 0).
+    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
+        sh.slot[lane] = slot;
+        if (lane == 0) sh.go = 1;
+        named_bar(1);
+        tasks(din);
+        named_bar(2);
+        const uint2 r0 = sh.out[0];
         const uint32_t c1 = r0.y & 0xffu;
-        uint2 r1 = s_out[1 + (c1 < cmax ? c1 : cmax)];
+        uint2 r1 = sh.out[1 + (c1 < cmax ? c1 : cmax)];
         if (c1 == dead) r1 = make_uint2(deadw, deadw);
         const uint32_t c2 = r1.y & 0xffu;
-        uint2 r2 = s_out[1 + nd + (c2 < cmax ? c2 : cmax)];
+        uint2 r2 = sh.out[1 + nd + (c2 < cmax ? c2 : cmax)];
         if (c2 == dead) r2 = make_uint2(deadw, deadw);
         const uint32_t c3 = r2.y & 0xffu;
-        uint2 r3 = s_out[1 + 2 * nd + (c3 < cmax ? c3 : cmax)];
+        uint2 r3 = sh.out[1 + 2 * nd + (c3 < cmax ? c3 : cmax)];
         if (c3 == dead) r3 = make_uint2(deadw, deadw);
         const uint2 row = seg == 0 ? r0 : seg == 1 ? r1 : seg == 2 ? r2 : r3;
         const uint32_t in = seg == 0 ? din : seg == 1 ? c1 : seg == 2 ? c2 : c3;
         const uint32_t pw = pos < 4 ? row.x : row.y;
-        const uint32_t sh = 24u - 8u * (uint32_t)(pos & 3);
-        d = (pw >> sh) & 0xffu;
+        const uint32_t shf = 24u - 8u * (uint32_t)(pos & 3);
+        d = (pw >> shf) & 0xffu;
         const uint32_t pm = pos <= 4 ? row.x : row.y;  // byte pos - 1
         const uint32_t shm = 24u - 8u * (uint32_t)((pos + 3) & 3);
         ctx = pos == 0 ? in : (pm >> shm) & 0xffu;
@@ -716,45 +749,51 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         r += (uint64_t)cnt;
         if (__any_sync(0xffffffffu, sawdead != 0)) status = FQXV_RANS_E_ABSENT_CONTEXT;
     }
+    // release the helper warps
+    if (lane == 0) sh.go = 0;
+    named_bar(1);
     return status;
 }
 
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(kO1Threads, 1)
     dec_o1d_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
                    uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ __align__(16) uint32_t s_slot[32];
-    __shared__ __align__(16) uint2 s_out[kOutRows + 1];
-    const int lane = threadIdx.x;
+    __shared__ __align__(16) O1Shared sh;
+    __shared__ int s_job;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t lt = lanemask_lt();
     TableStager st;
-    st.init(&bar);
+    if (warp == 0) st.init(&bar);
+    __syncthreads();
     for (;;) {
-        const int j = pop_job(queue);
+        if (tid == 0) s_job = atomicAdd(queue, 1);
+        __syncthreads();
+        const int j = s_job;
+        __syncthreads();
         if (j >= nlist) return;
         DecStream &S = streams[list[j]];
-        st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
         WordRing R;
-        R.init(src + S.words_off, S.words_len, sm + ring_off);
-        if (!st.wait()) {
-            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
-            st.wait();
-            return;
+        bool ok = true;
+        if (warp == 0) {
+            st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
+            R.init(src + S.words_off, S.words_len, sm + ring_off);
+            ok = st.wait();
+            if (!ok) {
+                if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
+                st.wait();
+            }
+            if (lane == 0) sh.go = ok;
         }
+        __syncthreads();  // the table image is visible to every warp
+        if (!sh.go) return;
         uint8_t *out = dst + S.dst_off;
-        const int tpl = (1 + 3 * S.nd + 31) / 32;
-        int status;
-        switch (tpl) {
-            case 1: status = o1d_stream<1>(S, sm, R, s_slot, s_out, out, lt); break;
-            case 2: status = o1d_stream<2>(S, sm, R, s_slot, s_out, out, lt); break;
-            case 3: status = o1d_stream<3>(S, sm, R, s_slot, s_out, out, lt); break;
-            case 4: status = o1d_stream<4>(S, sm, R, s_slot, s_out, out, lt); break;
-            default: status = o1d_stream<5>(S, sm, R, s_slot, s_out, out, lt); break;
-        }
-        if (lane == 0) S.status = status;
-        __syncwarp();
+        const int tpl = (1 + 3 * S.nd + kO1Threads - 1) / kO1Threads;
+        const int status = tpl <= 1 ? o1d_stream<1>(S, sm, R, sh, out, lt) : o1d_stream<2>(S, sm, R, sh, out, lt);
+        if (tid == 0) S.status = status;
+        __syncthreads();
     }
 }
 
@@ -868,7 +907,7 @@ void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint3
             break;
         case kClsO1Dense:
             cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
-            dec_o1d_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
+            dec_o1d_kernel<<<grid, kO1Threads, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
                                                         smem_bytes - kRingBytes);
             break;
         case kClsO1Global:

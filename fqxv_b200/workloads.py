@@ -153,14 +153,28 @@ def config1(nblocks: int = 64, block: int = MiB, seed: int = 0):
     return data, _spans([block] * nblocks)
 
 
-def config2(nblocks: int = 4096, lo: int = 4 * KiB, hi: int = 4 * MiB, seed: int = 0):
+def _gen_one(args):
+    name, size, seed = args
+    return GENERATORS[name](size, seed)
+
+
+def config2(nblocks: int = 4096, lo: int = 4 * KiB, hi: int = 4 * MiB, seed: int = 0, workers: int = 0):
     """Mixed blocks, sizes log-uniform in [lo, hi], stream type uniform over
-    the four generators; block i is seeded with seed + i."""
+    the four generators; block i is seeded with seed + i. `workers` > 1
+    generates blocks in a spawn-started process pool (the output is the same)."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), size=nblocks)).astype(np.int64)
     kinds = rng.integers(0, 4, size=nblocks)
     names = list(GENERATORS)
-    blocks = [GENERATORS[names[k]](int(s), seed + i) for i, (s, k) in enumerate(zip(sizes, kinds))]
+    jobs = [(names[k], int(s), seed + i) for i, (s, k) in enumerate(zip(sizes, kinds))]
+    if workers > 1 and nblocks > 64:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            blocks = list(ex.map(_gen_one, jobs, chunksize=16))
+    else:
+        blocks = [_gen_one(j) for j in jobs]
     data = np.concatenate(blocks) if blocks else np.zeros(0, np.uint8)
     return data, _spans(sizes), [names[k] for k in kinds]
 

@@ -175,6 +175,34 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
                                 size_t nblocks, uint64_t max_len, uint8_t *h_dst,
                                 const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status);
 
+/* ---- serving: continuous batching -----------------------------------------
+ * No reference counterpart. A server owns n_workers contexts (CUDA streams)
+ * on one device. Requests (one stream each) are admitted in arrival order
+ * while their device-memory estimate fits under hbm_cap (0: 40 GiB); a free
+ * worker takes every admitted request with the oldest request's kind and
+ * order mode and codes them as one batched pass, so requests arriving while
+ * others run join the next pass and passes of different workers overlap on
+ * the device. Results are byte-identical to the single calls. */
+typedef struct fqxv_rans_server fqxv_rans_server;
+
+int fqxv_rans_server_create(int device, int n_workers, uint64_t hbm_cap, fqxv_rans_server **out);
+/* Finishes queued work, then frees the server. */
+void fqxv_rans_server_destroy(fqxv_rans_server *server);
+/* kind 0: compress `src` with order mode `order`; kind 1: decompress `src`
+ * with decode_bounded's `max_len`. The bytes are copied; *id identifies the
+ * request. FQXV_RANS_E_TOO_LARGE when one request alone exceeds the cap. */
+int fqxv_rans_server_submit(fqxv_rans_server *server, int kind, const uint8_t *src, size_t len, int order,
+                            uint64_t max_len, uint64_t *id);
+/* Wait up to timeout_ms (-1: no limit) for request id. On completion returns
+ * FQXV_RANS_OK with its output length, its coding status and its latency
+ * (submit to completion, microseconds); FQXV_RANS_E_TIMEOUT if not done. */
+int fqxv_rans_server_wait(fqxv_rans_server *server, uint64_t id, int timeout_ms, size_t *out_len, int32_t *status,
+                          double *latency_us);
+/* Copy a completed request's output (cap >= its length) and release it. */
+int fqxv_rans_server_take(fqxv_rans_server *server, uint64_t id, uint8_t *dst, size_t cap);
+int fqxv_rans_server_stats(fqxv_rans_server *server, uint64_t *completed, uint64_t *batches,
+                           uint64_t *peak_bytes, uint64_t *pending);
+
 /* No counterpart in the reference. Encode one block that is already in device
  * memory without allocating any device memory, for callers that cannot call
  * cudaMalloc (a fixed device-memory budget reserved at start-up, an allocator

@@ -26,6 +26,14 @@ Layouts walked (all little-endian):
   (`crates/fqxv-tokenizer/src/lib.rs:98-103, 118-137, 176-200, 482-540`).
 * the reorder permutation frame, when non-empty, is one rANS stream
   (`crates/fqxv/src/container/reorder.rs:597-609`).
+* a sequence stream with method byte 4 is the long-read tile layout:
+  `LRT`, u8 version 1, varint n, varint total_bases, then `put_stream`
+  frames `[varint raw_len]([varint enc_len][rANS bytes] when raw_len > 0)`
+  for lens, markers, tile_lens, strands, rs, lit_lens, three range-coded
+  blobs `[varint count][varint len][bytes]` interleaved after lit_lens and
+  runs, then indel_lens, literals, exc_pos, exc_bytes
+  (`crates/fqxv-lroverlap/src/tile.rs:714-800`, `codec.rs:293-306`; the
+  `put_stream` rule keeps order-1 on a tie).
 
 Run here (where the reference tree is mounted):
     python tests/golden/make_golden.py /root/reference/crates/fqxv/tests/fixtures
@@ -87,6 +95,44 @@ def tokenizer_streams(names: bytes) -> list[tuple[str, bytes]]:
     return out
 
 
+def tile_streams(seq: bytes) -> list[tuple[str, bytes]]:
+    """rANS streams of a long-read tile sequence stream (method byte 4)."""
+    out: list[tuple[str, bytes]] = []
+    pos = 0
+    if seq[pos:pos + 3] != b"LRT" or seq[pos + 3] != 1:
+        raise ValueError("not a tile v1 stream")
+    pos += 4
+    _, pos = varint(seq, pos)  # n
+    _, pos = varint(seq, pos)  # total bases
+
+    def put(label: str) -> None:
+        nonlocal pos
+        raw_len, pos = varint(seq, pos)
+        if raw_len == 0:
+            return
+        ln, pos = varint(seq, pos)
+        out.append((label, seq[pos:pos + ln]))
+        pos += ln
+
+    def blob() -> None:
+        nonlocal pos
+        _, pos = varint(seq, pos)
+        ln, pos = varint(seq, pos)
+        pos += ln
+
+    for role in ("lens", "markers", "tile_lens", "strands", "rs", "lit_lens"):
+        put(role)
+    blob()  # ops
+    put("runs")
+    blob()  # subs
+    blob()  # ins
+    for role in ("indel_lens", "literals", "exc_pos", "exc_bytes"):
+        put(role)
+    if pos != len(seq):
+        raise ValueError("tile stream has %d trailing bytes" % (len(seq) - pos))
+    return out
+
+
 def header_len(buf: bytes) -> tuple[int, int]:
     if buf[:4] != b"FQXV":
         raise ValueError("bad magic")
@@ -112,6 +158,12 @@ def plain_streams(buf: bytes, pos: int) -> list[tuple[str, bytes]]:
         names = payload[p + 4:p + 4 + nlen]
         for role, s in tokenizer_streams(names):
             out.append(("block%d/%s" % (blk, role), s))
+        p += 4 + nlen
+        slen = struct.unpack_from("<I", payload, p)[0]
+        seq = payload[p + 4:p + 4 + slen]
+        if seq and seq[0] == 4:
+            for role, s in tile_streams(seq[1:]):
+                out.append(("block%d/seq_tile/%s" % (blk, role), s))
         blk += 1
     return out
 

@@ -11,7 +11,7 @@ import pytest
 # --- the pin: stored bytes from the reference's container fixtures --------
 
 def test_golden_streams_decode_and_reencode_identically(orc, golden):
-    assert len(golden) == 32
+    assert len(golden) == 41
     for meta, stream in golden:
         dec = orc.decode(stream)
         assert len(dec) == meta["n"]
