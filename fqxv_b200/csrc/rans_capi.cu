@@ -74,6 +74,8 @@ struct HostBuf {
     }
 };
 
+constexpr int kGroups = 6;  // decode launch groups
+
 enum Stage {
     kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
     kStages
@@ -149,8 +151,8 @@ struct fqxv_rans_ctx {
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
-    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};   // decode classes run side by side
-    cudaEvent_t ev_fork = nullptr, ev_join[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t aux[kGroups] = {};   // decode launch groups run side by side
+    cudaEvent_t ev_fork = nullptr, ev_join[kGroups] = {};
     std::mutex mu;
     // encode
     DevBuf e_blocks, e_order, e_jobs, e_tbl, e_words, e_hist, e_misc;
@@ -366,7 +368,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     CK(ctx->d_streams.ensure(nb * sizeof(DecStream), s));
     CK(ctx->d_order.ensure(nb * 4, s));
     CK(ctx->d_tbl.ensure(std::max<uint64_t>(toff, 256), s));
-    CK(ctx->d_misc.ensure(256, s));
+    CK(ctx->d_misc.ensure(512, s));
     const size_t szs = nb * sizeof(DecStream), szo = nb * 4;
     CK(ctx->h_stage.ensure(szs + szo + 64));
     cudaStreamSynchronize(s);
@@ -396,57 +398,67 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     CK(cudaMemcpyAsync(hst, dS, szs, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     {
+        // Launch groups: order-0; order-1 dense by alphabet size (the shared
+        // memory of a group is its largest member's, so small alphabets get
+        // many CTAs per SM); order-1 global.
         const DecStream *ps = reinterpret_cast<const DecStream *>(hst);
-        std::vector<uint32_t> lists[3];
-        uint32_t smem[3] = {0, 0, 0};
-        uint64_t cbytes[3] = {0, 0, 0};
+        auto group_of = [&](const DecStream &d) -> int {
+            if (d.cls == kClsO0) return 0;
+            if (d.cls == kClsO1Global) return kGroups - 1;
+            if (d.cls != kClsO1Dense) return -1;
+            return d.nd <= 7 ? 1 : d.nd <= 15 ? 2 : d.nd <= 31 ? 3 : 4;
+        };
+        std::vector<uint32_t> lists[kGroups];
+        uint32_t smem[kGroups] = {};
+        uint64_t cbytes[kGroups] = {};
         for (uint32_t i : ord) {
-            const int c = ps[i].cls;
-            if (c < kClsO0 || c > kClsO1Global) continue;
-            lists[c - kClsO0].push_back(i);
-            smem[c - kClsO0] = std::max(smem[c - kClsO0], dec_smem_bytes(c, ps[i].nd));
-            cbytes[c - kClsO0] += ps[i].src_len + ps[i].n;
+            const int g = group_of(ps[i]);
+            if (g < 0) continue;
+            lists[g].push_back(i);
+            smem[g] = std::max(smem[g], dec_smem_bytes(ps[i].cls, ps[i].nd));
+            cbytes[g] += ps[i].src_len + ps[i].n;
         }
-        size_t tot = lists[0].size() + lists[1].size() + lists[2].size();
+        size_t tot = 0;
+        for (int g = 0; g < kGroups; g++) tot += lists[g].size();
         CK(ctx->d_order.ensure(std::max<size_t>(tot, 1) * 4, s));
         uint32_t *hl = reinterpret_cast<uint32_t *>(hst + szs);
-        size_t at = 0, base[3];
-        for (int c = 0; c < 3; c++) {
-            base[c] = at;
-            std::memcpy(hl + at, lists[c].data(), lists[c].size() * 4);
-            at += lists[c].size();
+        size_t at = 0, base[kGroups];
+        for (int g = 0; g < kGroups; g++) {
+            base[g] = at;
+            std::memcpy(hl + at, lists[g].data(), lists[g].size() * 4);
+            at += lists[g].size();
         }
         if (tot) CK(cudaMemcpyAsync(ctx->d_order.p, hl, tot * 4, cudaMemcpyHostToDevice, s));
-        CK(cudaMemsetAsync(queue, 0, 64, s));
+        CK(cudaMemsetAsync(queue, 0, 4 * 4 * kGroups, s));
         CK(cudaEventRecord(ctx->ev_fork, s));
         const uint32_t *dl = ctx->d_order.as<uint32_t>();
-        const int st_of[3] = {kStDecO0, kStDecO1Dense, kStDecO1Global};
-        for (int c = 0; c < 3; c++) {
-            const size_t m = lists[c].size();
+        for (int g = 0; g < kGroups; g++) {
+            const size_t m = lists[g].size();
             if (!m) continue;
-            cudaStream_t as = ctx->aux[c];
+            const int cls = g == 0 ? kClsO0 : g == kGroups - 1 ? kClsO1Global : kClsO1Dense;
+            const int stage = g == 0 ? kStDecO0 : g == kGroups - 1 ? kStDecO1Global : kStDecO1Dense;
+            cudaStream_t as = ctx->aux[g];
             CK(cudaStreamWaitEvent(as, ctx->ev_fork, 0));
-            const uint32_t sm_b = smem[c] + 2048;  // + static shared memory and per-CTA reserve
+            const uint32_t sm_b = smem[g] + 2048;  // + static shared memory and per-CTA reserve
             int per_sm = (int)(233472u / sm_b);
-            per_sm = std::max(1, std::min(per_sm, 32));
+            per_sm = std::max(1, std::min(per_sm, cls == kClsO1Dense ? 8 : 32));
             if (persistent) {
                 const int grid = (int)std::min<size_t>(m, (size_t)ctx->sms * per_sm);
                 cudaEvent_t t0 = ctx->timer.begin(as);
-                launch_dec_run(kClsO0 + c, d_src, dS, dl + base[c], (int)m, dT, d_dst, queue + 4 * c, grid,
-                               smem[c], as);
-                ctx->timer.end(st_of[c], t0, as);
+                launch_dec_run(cls, d_src, dS, dl + base[g], (int)m, dT, d_dst, queue + 4 * g, grid, smem[g], as);
+                ctx->timer.end(stage, t0, as);
             } else {
                 for (size_t j = 0; j < m; j++) {
-                    CK(cudaMemsetAsync(queue + 4 * c, 0, 4, as));
+                    CK(cudaMemsetAsync(queue + 4 * g, 0, 4, as));
                     cudaEvent_t t0 = ctx->timer.begin(as);
-                    launch_dec_run(kClsO0 + c, d_src, dS, dl + base[c] + j, 1, dT, d_dst, queue + 4 * c, 1,
-                                   dec_smem_bytes(kClsO0 + c, ps[lists[c][j]].nd), as);
-                    ctx->timer.end(st_of[c], t0, as);
+                    launch_dec_run(cls, d_src, dS, dl + base[g] + j, 1, dT, d_dst, queue + 4 * g, 1,
+                                   dec_smem_bytes(cls, ps[lists[g][j]].nd), as);
+                    ctx->timer.end(stage, t0, as);
                 }
             }
-            ctx->timer.bytes[st_of[c]] += cbytes[c];
-            CK(cudaEventRecord(ctx->ev_join[c], as));
-            CK(cudaStreamWaitEvent(s, ctx->ev_join[c], 0));
+            ctx->timer.bytes[stage] += cbytes[g];
+            CK(cudaEventRecord(ctx->ev_join[g], as));
+            CK(cudaStreamWaitEvent(s, ctx->ev_join[g], 0));
         }
     }
     CK(cudaGetLastError());
@@ -530,7 +542,7 @@ int fqxv_rans_ctx_create(int device, fqxv_rans_ctx **out) {
     c->sms = sm_count(device);
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess;
-    for (int i = 0; i < 3 && ok; i++)
+    for (int i = 0; i < kGroups && ok; i++)
         ok = cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
@@ -553,7 +565,7 @@ void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
     ctx->h_stage.release();
     ctx->h_io.release();
     ctx->timer.release();
-    for (int i = 0; i < 3; i++) {
+    for (int i = 0; i < kGroups; i++) {
         if (ctx->aux[i]) cudaStreamDestroy(ctx->aux[i]);
         if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
     }
