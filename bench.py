@@ -43,18 +43,23 @@ METRIC = "rANS Nx16 enc/dec GB/s, bit-exact (uncompressed bytes per second, enco
 L2_FLUSH_BYTES = 256 << 20
 
 
-def build_workload(name: str, seed: int):
-    """-> (data u8, spans (n,2), encode order or None for decode-only, description, extra)."""
+def build_workload(name: str, seed: int, blocks: int = 0):
+    """-> (data u8, spans (n,2), encode order or None for decode-only, description, extra).
+
+    `blocks` > 0 shrinks configs 1 and 2 to that many blocks (small cases for
+    profiler captures); 0 keeps the benchmark shape."""
     if name == "config1":
-        data, spans = W.config1(seed=seed)
-        return data, spans, 1, "64 x 1 MiB full-range quality blocks, order-1", {}
+        nb = blocks or 64
+        data, spans = W.config1(nblocks=nb, seed=seed)
+        return data, spans, 1, "%d x 1 MiB full-range quality blocks, order-1" % nb, {}
     if name == "config0":
         data, spans = W.config0(seed=seed)
         return data, spans, 0, "1 x 1 MiB binned quality block, order-0", {}
     workers = min(32, os.cpu_count() or 1)
     if name == "config2":
-        data, spans, kinds = W.config2(seed=seed, workers=workers)
-        return data, spans, 2, "4096 mixed blocks 4 KiB-4 MiB, both orders, keep the smaller", {}
+        nb = blocks or 4096
+        data, spans, kinds = W.config2(nblocks=nb, seed=seed, workers=workers)
+        return data, spans, 2, "%d mixed blocks 4 KiB-4 MiB, both orders, keep the smaller" % nb, {}
     if name == "config3":
         d2, s2, _ = W.config2(seed=seed, workers=workers)
         d3, s3 = W.config3_ont(seed=seed)
@@ -162,7 +167,7 @@ def cpu_encoded(data, spans, seed_tag):
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
-    data, spans, order, desc, extra = build_workload(args.workload, args.seed)
+    data, spans, order, desc, extra = build_workload(args.workload, args.seed, args.blocks)
     nthreads = os.cpu_count() or 1
     n_bytes = int(spans[:, 1].sum())
     from oracle import oracle
@@ -330,6 +335,8 @@ def main() -> None:
     ap.add_argument("--workers", type=int, default=4, help="config4: server workers (streams)")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--blocks", type=int, default=0,
+                    help="configs 1/2: number of blocks (0 = the benchmark shape; smaller for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
@@ -362,7 +369,7 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    data, spans, order, desc, extra = build_workload(args.workload, args.seed + rank)
+    data, spans, order, desc, extra = build_workload(args.workload, args.seed + rank, args.blocks)
     n_bytes = int(spans[:, 1].sum())
     codec = Codec(local)
     cs = torch.cuda.ExternalStream(codec.stream_handle)
@@ -437,11 +444,14 @@ def main() -> None:
     pk = peaks()
     timed = {k: v for k, v in stages.items() if v["launches"] > 0}
     dom = max(timed, key=lambda k: timed[k]["ms"])
-    per_launch_ms = timed[dom]["ms"] / timed[dom]["launches"]
-    # Algorithmic bytes of one launch: the coder reads its input once and
-    # writes its output once -- n + compressed for the run/model kernels of a
-    # batch (tables are on chip and excluded).
-    alg_bytes = n_bytes + comp_bytes
+    launches = timed[dom]["launches"]
+    per_launch_ms = timed[dom]["ms"] / launches
+    # Algorithmic bytes of a launch: the stage reads its input once and writes
+    # its output once (decode: compressed + n of the streams it decodes;
+    # encode: n + the words written); tables are on chip and excluded. The
+    # library accumulates them per stage, so a stage split over several
+    # launches (decode groups) divides them by its launch count.
+    alg_bytes = timed[dom]["bytes"] / launches
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
@@ -453,7 +463,7 @@ def main() -> None:
             traffic = ent.get("dram_bytes_per_launch")
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 5), "traffic": traffic,
-                "alg_bytes_per_launch": alg_bytes, "launch_ms": round(per_launch_ms, 4),
+                "alg_bytes_per_launch": int(alg_bytes), "launch_ms": round(per_launch_ms, 4),
                 "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"}
     gpu_launches = int(sum(v["launches"] for v in stages.values()))
 
@@ -549,7 +559,8 @@ def main() -> None:
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": gpu_launches,
-            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4)} for k, v in stages.items()},
+            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "bytes": v["bytes"]}
+                       for k, v in stages.items()},
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
