@@ -439,8 +439,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             const int stage = g == 0 ? kStDecO0 : g == kGroups - 1 ? kStDecO1Global : kStDecO1Dense;
             cudaStream_t as = ctx->aux[g];
             CK(cudaStreamWaitEvent(as, ctx->ev_fork, 0));
-            const uint32_t sm_b = smem[g] + 2048;  // + static shared memory and per-CTA reserve
-            int per_sm = (int)(233472u / sm_b);
+            int per_sm = dec_blocks_per_sm(cls, smem[g]);
             per_sm = std::max(1, std::min(per_sm, cls == kClsO1Dense ? 8 : 32));
             if (persistent) {
                 const int grid = (int)std::min<size_t>(m, (size_t)ctx->sms * per_sm);

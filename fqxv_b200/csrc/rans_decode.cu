@@ -553,12 +553,15 @@ __global__ void __launch_bounds__(32)
 //
 // Per round, the context chain d_i = chain[d_{i-1}][slot_i] of the 32 lanes
 // is resolved in four segments of eight: segment 0 from the known incoming
-// context, segments 1-3 for every possible incoming context (tasks
-// 1 + (k-1) nd + c), then three dependent lookups pick the real rows. The
-// 1 + 3 nd eight-step chains are spread over all 128 threads (TPL per thread,
-// a template parameter), so the stream's SM runs them on all four schedulers.
-// Warp 0 owns the 32 states, the renorm words and the output; the other warps
-// only run chains. Two named barriers per round: slots ready, rows ready.
+// context, segments 1-3 for every possible incoming context at once, then
+// three dependent lookups pick the real rows. Every warp holds its own copy
+// of the 32 states, the word position and the incoming context, and runs the
+// same renormalisation on the same words (from its own word ring), so the
+// copies never diverge and one barrier per round suffices: each thread runs
+// its share of the 3 nd speculative chains (TPL per thread, a template
+// parameter) plus, on lane 0 of every warp, segment 0; the rows go to a
+// double-buffered shared array, and after the barrier every warp resolves
+// the round itself. Only warp 0 stores the output.
 //
 // Rounds that cannot run out of words (and are not the first or the partial
 // last round) take a branch-free fast path: the ring advances by predication,
@@ -568,45 +571,73 @@ __global__ void __launch_bounds__(32)
 // every check of scalar.rs:202-215 in order.
 constexpr int kO1Warps = 4;
 constexpr int kO1Threads = 32 * kO1Warps;
+constexpr int kO1Workers = kO1Threads - kO1Warps;  // threads that run speculative chains
 
 __device__ __forceinline__ void named_bar(int id) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kO1Threads) : "memory");
 }
 
-struct O1Shared {
-    uint32_t slot[32];
-    uint2 out[kOutRows + 1];
-    uint32_t din;
-    int go;
-};
+// Rows of the speculative chains, 16 bytes each: the eight chain values
+// (d_0 the top byte of .x, d_7 the low byte of .y) and, in .z, the byte
+// offset of the row the next segment continues from (the DEAD row when the
+// chain ends in a context without a table), so that resolving a round is
+// three dependent loads and no index arithmetic. Row kDeadRow repeats DEAD;
+// row kPadRow takes the stores of threads without a task.
+constexpr uint32_t kDeadRow = 3 * kDenseMax;
+constexpr uint32_t kPadRow = kDeadRow + 1;
+static_assert(kPadRow <= kOutRows, "row array too small");
 
 template <int TPL>
 __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
-                                          O1Shared &sh, uint8_t *__restrict__ out, uint32_t lt) {
+                                          uint4 (*__restrict__ rows)[kOutRows + 1], uint8_t *__restrict__ out,
+                                          uint32_t lt) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nd = S.nd;
     const uint32_t dead = (uint32_t)nd;
-    const int ntask = 1 + 3 * nd;
-    uint32_t seg_q[TPL], c_q[TPL], idx_q[TPL];
+    const int nspec = 3 * nd;
+    // This thread's chains: lane 0 of each warp runs segment 0 (q = 0); the
+    // other threads split the speculative tasks u = (seg - 1) nd + c.
+    const int worker = warp * 31 + lane - 1;
+    uint32_t seg_q[TPL], c_q[TPL], idx_q[TPL], nbase_q[TPL];
 #pragma unroll
     for (int q = 0; q < TPL; q++) {
-        const int t = tid + kO1Threads * q;
-        const bool valid = t < ntask;
-        seg_q[q] = (!valid || t == 0) ? 0u : (uint32_t)(1 + (t - 1) / nd);
-        c_q[q] = (!valid || t == 0) ? 0u : (uint32_t)((t - 1) % nd);
-        idx_q[q] = !valid ? kOutRows : (t == 0 ? 0u : 1u + (seg_q[q] - 1) * (uint32_t)nd + c_q[q]);
+        const int u = worker + kO1Workers * q;
+        const bool valid = lane != 0 && u < nspec;
+        seg_q[q] = lane == 0 ? 0u : valid ? (uint32_t)(1 + u / nd) : 1u;
+        c_q[q] = valid ? (uint32_t)(u % nd) : 0u;
+        idx_q[q] = valid ? (uint32_t)u : kPadRow;
+        nbase_q[q] = seg_q[q] * (uint32_t)nd;  // first row of the next segment
     }
     const uint8_t *CT = sm;
-    // Chain rows of this round for this thread's tasks. Row bytes: d_0 is the
-    // top byte of .x, d_7 the low byte of .y.
-    auto tasks = [&](uint32_t din) {
-        uint2 rows[TPL];
+    const uint32_t stride = (uint32_t)nd + 1;
+    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
+    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
+    const uint32_t deadw = 0x01010101u * dead;
+    if (tid == 0) {
+        rows[0][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
+        rows[1][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
+    }
+    const uint64_t n = S.n;
+    const uint64_t navail = S.words_len / 2;
+    uint32_t x = S.states[lane];
+    uint64_t wp = 0;
+    uint32_t din = (uint32_t)S.start;
+    const uint64_t rounds = (n + 31) / 32, full = n / 32;
+    const int seg = lane >> 3, pos = lane & 7;
+    const uint32_t shd = 24u - 8u * (uint32_t)(pos & 3);        // byte pos of a row half
+    const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);  // byte pos - 1
+    uint32_t buf = 0;
+
+    // One round: the chains of this thread, the barrier, then the resolved
+    // symbol d and context ctx of this lane.
+    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
+        uint4 mine[TPL];
 #pragma unroll
         for (int q = 0; q < TPL; q++) {
-            const uint4 sa = *reinterpret_cast<const uint4 *>(sh.slot + 8 * seg_q[q]);
-            const uint4 sb = *reinterpret_cast<const uint4 *>(sh.slot + 8 * seg_q[q] + 4);
-            const uint32_t sl[8] = {sa.x, sa.y, sa.z, sa.w, sb.x, sb.y, sb.z, sb.w};
-            uint32_t dd = (q == 0 && tid == 0) ? din : c_q[q];
+            uint32_t sl[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, slot, 8 * seg_q[q] + k);
+            uint32_t dd = (q == 0 && lane == 0) ? din : c_q[q];
             uint32_t hi = 0, lo = 0;
 #pragma unroll
             for (int k = 0; k < 4; k++) {
@@ -618,64 +649,31 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
                 dd = CT[dd * kChainStride + sl[k]];
                 lo = lo * 256u + dd;
             }
-            rows[q] = make_uint2(hi, lo);
+            mine[q] = make_uint4(hi, lo, 16u * (dd == dead ? kDeadRow : nbase_q[q] + dd), 0u);
         }
+        uint4 *rb = rows[buf];
 #pragma unroll
-        for (int q = 0; q < TPL; q++) sh.out[idx_q[q]] = rows[q];
-    };
-
-    if (warp != 0) {
-        // helper warps: run this thread's chains every round until told to stop
-        for (;;) {
-            named_bar(1);
-            if (!sh.go) break;
-            tasks(0);
-            named_bar(2);
-        }
-        return FQXV_RANS_OK;
-    }
-
-    const uint32_t stride = (uint32_t)nd + 1;
-    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
-    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
-    const uint32_t deadw = 0x01010101u * dead;
-    const uint32_t cmax = nd > 0 ? (uint32_t)nd - 1 : 0u;
-    const uint64_t n = S.n;
-    const uint64_t navail = S.words_len / 2;
-    uint32_t x = S.states[lane];
-    uint64_t wp = 0;
-    uint32_t din = (uint32_t)S.start;
-    const uint64_t rounds = (n + 31) / 32, full = n / 32;
-    const int seg = lane >> 3, pos = lane & 7;
-
-    // One round of chains across the CTA, then the resolved symbol d and
-    // context ctx of this lane (warp 0).
-    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
-        sh.slot[lane] = slot;
-        if (lane == 0) sh.go = 1;
+        for (int q = 0; q < TPL; q++)
+            if (q > 0 || lane != 0) rb[idx_q[q]] = mine[q];
+        uint4 r0;
+        r0.x = __shfl_sync(0xffffffffu, mine[0].x, 0);
+        r0.y = __shfl_sync(0xffffffffu, mine[0].y, 0);
+        r0.z = __shfl_sync(0xffffffffu, mine[0].z, 0);
         named_bar(1);
-        tasks(din);
-        named_bar(2);
-        const uint2 r0 = sh.out[0];
-        const uint32_t c1 = r0.y & 0xffu;
-        uint2 r1 = sh.out[1 + (c1 < cmax ? c1 : cmax)];
-        if (c1 == dead) r1 = make_uint2(deadw, deadw);
-        const uint32_t c2 = r1.y & 0xffu;
-        uint2 r2 = sh.out[1 + nd + (c2 < cmax ? c2 : cmax)];
-        if (c2 == dead) r2 = make_uint2(deadw, deadw);
-        const uint32_t c3 = r2.y & 0xffu;
-        uint2 r3 = sh.out[1 + 2 * nd + (c3 < cmax ? c3 : cmax)];
-        if (c3 == dead) r3 = make_uint2(deadw, deadw);
-        const uint2 row = seg == 0 ? r0 : seg == 1 ? r1 : seg == 2 ? r2 : r3;
-        const uint32_t in = seg == 0 ? din : seg == 1 ? c1 : seg == 2 ? c2 : c3;
-        const uint32_t pw = pos < 4 ? row.x : row.y;
-        const uint32_t shf = 24u - 8u * (uint32_t)(pos & 3);
-        d = (pw >> shf) & 0xffu;
-        const uint32_t pm = pos <= 4 ? row.x : row.y;  // byte pos - 1
-        const uint32_t shm = 24u - 8u * (uint32_t)((pos + 3) & 3);
-        ctx = pos == 0 ? in : (pm >> shm) & 0xffu;
+        const uint8_t *rbb = reinterpret_cast<const uint8_t *>(rb);
+        const uint4 r1 = *reinterpret_cast<const uint4 *>(rbb + r0.z);
+        const uint4 r2 = *reinterpret_cast<const uint4 *>(rbb + r1.z);
+        const uint32_t rx = seg == 0 ? r0.x : seg == 1 ? r1.x : r2.x;
+        const uint32_t ry = seg == 0 ? r0.y : seg == 1 ? r1.y : r2.y;
+        const uint32_t ine = seg == 0 ? din : seg == 1 ? (r0.y & 0xffu) : (r1.y & 0xffu);
+        const uint4 r3 = *reinterpret_cast<const uint4 *>(rbb + r2.z);
+        const uint32_t row_x = seg == 3 ? r3.x : rx;
+        const uint32_t row_y = seg == 3 ? r3.y : ry;
+        const uint32_t in = seg == 3 ? (r2.y & 0xffu) : ine;
+        d = ((pos < 4 ? row_x : row_y) >> shd) & 0xffu;
+        ctx = pos == 0 ? in : ((pos <= 4 ? row_x : row_y) >> shc) & 0xffu;
         din = r3.y & 0xffu;
-        __syncwarp();
+        buf ^= 1u;
     };
 
     uint64_t r = 0;
@@ -708,7 +706,7 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
                 break;
             }
             if (active) {
-                out[i] = DS[d];
+                if (warp == 0) out[i] = DS[d];
                 x = v;
             }
             r++;
@@ -740,7 +738,7 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
             const bool need = v < kRansL;
             const uint32_t mask = __ballot_sync(0xffffffffu, need);
             const uint32_t w = __shfl_sync(0xffffffffu, cand, __popc(mask & lt) & 31);
-            *op = DS[d];
+            if (warp == 0) *op = DS[d];
             op += 32;
             x = need ? (v << 16) | w : v;
             w32 += __popc(mask);
@@ -749,9 +747,6 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         r += (uint64_t)cnt;
         if (__any_sync(0xffffffffu, sawdead != 0)) status = FQXV_RANS_E_ABSENT_CONTEXT;
     }
-    // release the helper warps
-    if (lane == 0) sh.go = 0;
-    named_bar(1);
     return status;
 }
 
@@ -761,8 +756,8 @@ __global__ void __launch_bounds__(kO1Threads, 1)
                    uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ __align__(16) O1Shared sh;
-    __shared__ int s_job;
+    __shared__ __align__(16) uint4 s_rows[2][kOutRows + 1];
+    __shared__ int s_job, s_ok;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t lt = lanemask_lt();
     TableStager st;
@@ -775,23 +770,24 @@ __global__ void __launch_bounds__(kO1Threads, 1)
         __syncthreads();
         if (j >= nlist) return;
         DecStream &S = streams[list[j]];
-        WordRing R;
-        bool ok = true;
         if (warp == 0) {
             st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
-            R.init(src + S.words_off, S.words_len, sm + ring_off);
-            ok = st.wait();
+            const bool ok = st.wait();
             if (!ok) {
                 if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
                 st.wait();
             }
-            if (lane == 0) sh.go = ok;
+            if (lane == 0) s_ok = ok;
         }
+        // every warp reads the words through its own ring
+        WordRing R;
+        R.init(src + S.words_off, S.words_len, sm + ring_off + warp * kRingBytes);
         __syncthreads();  // the table image is visible to every warp
-        if (!sh.go) return;
+        if (!s_ok) return;
         uint8_t *out = dst + S.dst_off;
-        const int tpl = (1 + 3 * S.nd + kO1Threads - 1) / kO1Threads;
-        const int status = tpl <= 1 ? o1d_stream<1>(S, sm, R, sh, out, lt) : o1d_stream<2>(S, sm, R, sh, out, lt);
+        const int tpl = (3 * S.nd + kO1Workers - 1) / kO1Workers;
+        const int status = tpl <= 1 ? o1d_stream<1>(S, sm, R, s_rows, out, lt)
+                                    : o1d_stream<2>(S, sm, R, s_rows, out, lt);
         if (tid == 0) S.status = status;
         __syncthreads();
     }
@@ -884,10 +880,36 @@ __global__ void __launch_bounds__(32)
 uint32_t dec_smem_bytes(int cls, int nd) {
     switch (cls) {
         case kClsO0: return 16384 + kRingBytes;
-        case kClsO1Dense: return (uint32_t)align_up(dense_table_bytes(nd), 128) + kRingBytes;
+        case kClsO1Dense: return (uint32_t)align_up(dense_table_bytes(nd), 128) + kO1Warps * kRingBytes;
         case kClsO1Global: return kRingBytes;
         default: return 0;
     }
+}
+
+int dec_blocks_per_sm(int cls, uint32_t smem_bytes) {
+    int n = 0;
+    cudaError_t e = cudaSuccess;
+    switch (cls) {
+        case kClsO0:
+            cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o0_kernel, 32, smem_bytes);
+            break;
+        case kClsO1Dense:
+            cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1d_kernel, kO1Threads, smem_bytes);
+            break;
+        case kClsO1Global:
+            cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1g_kernel, 32, smem_bytes);
+            break;
+        default:
+            break;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
 }
 
 void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint8_t *tbl, int grid,
@@ -908,7 +930,7 @@ void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint3
         case kClsO1Dense:
             cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
             dec_o1d_kernel<<<grid, kO1Threads, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                        smem_bytes - kRingBytes);
+                                                        smem_bytes - kO1Warps * kRingBytes);
             break;
         case kClsO1Global:
             cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
