@@ -1,12 +1,18 @@
 // Serving runtime: requests arrive one at a time (compress or decompress of
 // one stream), are admitted while their device-memory estimate fits under a
 // cap, and are coded in continuous batches: every worker owns a context (its
-// own CUDA stream and arenas); whenever a worker is free it takes all admitted
-// requests that share the oldest request's kind and order mode and runs them
-// as one batched pass, so requests that arrive while others are on the GPU
-// join the next pass of any free worker and passes of different workers
-// overlap on the device. No reference counterpart (the reference is a
-// library called per stream); results are byte-identical to the single calls.
+// own CUDA stream, device arenas and pinned staging); whenever a worker is
+// free it takes all admitted requests that share the oldest request's kind,
+// order mode and size class (sizes within a factor of four) and runs them as
+// one batched pass, so requests that arrive while others are on the GPU join
+// the next pass of any free worker, passes of different workers overlap on
+// the device, and a small request never waits for a large one in its own
+// pass. One stream is coded serially (its 32 states advance round by round),
+// so a request's latency is at least its own stream's; the runtime only
+// keeps queueing from adding to it. No reference counterpart (the reference
+// is a library called per stream); results are byte-identical to the single
+// calls.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -26,6 +32,7 @@ using Clock = std::chrono::steady_clock;
 struct Request {
     uint64_t id = 0;
     int kind = 0;          // 0 encode, 1 decode
+    int size_class = 0;    // floor(log4(input bytes))
     int order = 0;         // encode order mode
     uint64_t max_len = 0;  // decode bound
     std::vector<uint8_t> in;
@@ -45,7 +52,7 @@ struct HostPinned {
         if (p) cudaFreeHost(p);
         p = nullptr;
         cap = 0;
-        size_t nc = want + want / 4 + (1 << 20);
+        size_t nc = std::max(want, 2 * cap) + (1 << 20);
         if (cudaHostAlloc(&p, nc, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             return false;
@@ -57,6 +64,15 @@ struct HostPinned {
         if (p) cudaFreeHost(p);
     }
 };
+
+int size_class(size_t n) {
+    int b = 0;
+    while (n > 1) {
+        n >>= 1;
+        b++;
+    }
+    return b / 2;
+}
 
 uint64_t request_mem(const Request &r) {
     // Inputs, outputs and the per-block scratch of the batched passes.
@@ -83,14 +99,50 @@ struct fqxv_rans_server {
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
     std::vector<fqxv_rans_ctx *> ctxs;
     std::vector<std::thread> workers;
+    int warmed = 0;
 
     void worker(int w);
 };
+
+namespace {
+
+// Bring a worker to serving state before the first request: pinned staging
+// of a useful size, and one small pass of each kernel path (order-0 and
+// order-1 encode and decode) so module loading, kernel attributes and the
+// context's device arenas are in place.
+void warm_worker(fqxv_rans_ctx *ctx, HostPinned &h_in, HostPinned &h_out) {
+    const size_t n = 1 << 16;
+    if (!h_in.ensure(32u << 20) || !h_out.ensure(32u << 20)) return;
+    uint8_t *src = static_cast<uint8_t *>(h_in.p);
+    uint32_t z = 12345;
+    for (size_t i = 0; i < n; i++) {
+        z = z * 1103515245u + 12345u;
+        src[i] = (uint8_t)('A' + ((z >> 16) % 5));
+    }
+    uint8_t *enc = static_cast<uint8_t *>(h_out.p);
+    uint8_t *dec = src + n;
+    for (int order = FQXV_RANS_ORDER0; order <= FQXV_RANS_ORDER1; order++) {
+        fqxv_rans_span sp{0, n}, out{0, 0}, dsp{0, n};
+        int32_t ord = 0, st = 0;
+        uint64_t len = 0;
+        const uint64_t bound = fqxv_rans_encode_batch_bound(&sp, 1, order);
+        if (fqxv_rans_encode_batch_host(ctx, src, &sp, 1, order, enc, bound, &out, &ord) != FQXV_RANS_OK) return;
+        fqxv_rans_decode_batch_host(ctx, enc, &out, 1, n, dec, &dsp, &len, &st);
+    }
+}
+
+}  // namespace
 
 void fqxv_rans_server::worker(int w) {
     cudaSetDevice(device);
     fqxv_rans_ctx *ctx = ctxs[w];
     HostPinned h_in, h_out;
+    warm_worker(ctx, h_in, h_out);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        warmed++;
+    }
+    cv_done.notify_all();
     std::vector<Request *> batch;
     std::vector<fqxv_rans_span> spans, outs;
     std::vector<int32_t> orders, sts;
@@ -109,12 +161,12 @@ void fqxv_rans_server::worker(int w) {
             if (stop && pending.empty()) return;
             if (pending.empty()) continue;
             const int kind = pending.front()->kind, order = pending.front()->order;
-            const uint64_t max_len = pending.front()->max_len;
+            const int cls = pending.front()->size_class;
             size_t bytes = 0;
             // Continuous batching: everything admissible of the head's shape.
             for (auto it = pending.begin(); it != pending.end();) {
                 Request *r = *it;
-                const bool same = r->kind == kind && (kind == 1 ? r->max_len == max_len : r->order == order);
+                const bool same = r->kind == kind && r->size_class == cls && (kind == 1 || r->order == order);
                 const bool fits = (in_use + bmem == 0) || in_use + bmem + r->mem <= cap;
                 if (same && fits && (batch.empty() || bytes + r->in.size() <= max_batch_bytes)) {
                     batch.push_back(r);
@@ -165,9 +217,13 @@ void fqxv_rans_server::worker(int w) {
                     tout += batch[i]->n_out;
                 }
                 if (!h_out.ensure(tout + 16)) st = FQXV_RANS_E_OUT_OF_MEMORY;
+                uint64_t max_len = 0;
+                for (size_t i = 0; i < nb; i++) max_len = std::max(max_len, batch[i]->max_len);
                 if (st == FQXV_RANS_OK) {
+                    // Every member's declared length was checked against its
+                    // own bound at submission, so the pass may use the largest.
                     const int first = fqxv_rans_decode_batch_host(ctx, (const uint8_t *)h_in.p, spans.data(), nb,
-                                                                  batch[0]->max_len, (uint8_t *)h_out.p,
+                                                                  max_len, (uint8_t *)h_out.p,
                                                                   outs.data(), lens.data(), sts.data());
                     if (first > FQXV_RANS_E_TRUNCATED_RENORM) {
                         for (size_t i = 0; i < nb; i++) sts[i] = first;
@@ -219,6 +275,10 @@ int fqxv_rans_server_create(int device, int n_workers, uint64_t hbm_cap, fqxv_ra
         s->ctxs.push_back(c);
     }
     for (int i = 0; i < n_workers; i++) s->workers.emplace_back([s, i] { s->worker(i); });
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_done.wait(lk, [&] { return s->warmed == n_workers; });
+    }
     *out = s;
     return FQXV_RANS_OK;
 }
@@ -244,14 +304,32 @@ int fqxv_rans_server_submit(fqxv_rans_server *s, int kind, const uint8_t *src, s
     r->order = kind == 0 ? order : 0;
     r->max_len = kind == 1 ? max_len : 0;
     r->in.assign(src, src + len);
+    r->size_class = size_class(len);
+    bool bound_exceeded = false;
     if (kind == 1) {
         uint64_t n = 0;
         // A stream too short for a header decodes to an error; reserve nothing.
-        if (fqxv_rans_peek_output_len(src, len, &n) == FQXV_RANS_OK && n <= max_len) r->n_out = n;
+        if (fqxv_rans_peek_output_len(src, len, &n) == FQXV_RANS_OK) {
+            if (n <= max_len) r->n_out = n;
+            else bound_exceeded = true;  // lib.rs:227: rejected before decoding
+        }
     }
     r->mem = request_mem(*r);
     if (r->mem > s->cap) return FQXV_RANS_E_TOO_LARGE;
     r->t_submit = Clock::now();
+    if (bound_exceeded) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r->id = s->next_id++;
+        *id = r->id;
+        r->status = FQXV_RANS_E_BOUND;
+        r->done = true;
+        r->t_done = r->t_submit;
+        std::vector<uint8_t>().swap(r->in);
+        s->completed++;
+        s->all.emplace(r->id, std::move(r));
+        s->cv_done.notify_all();
+        return FQXV_RANS_OK;
+    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         r->id = s->next_id++;

@@ -1,14 +1,15 @@
 """Serving front end: continuous batching of compress / decompress requests
 on one GPU (the C++ runtime in csrc/rans_server.cu).
 
-    with Server(device=0, workers=4, hbm_cap=40 << 30) as srv:
+    with Server(device=0, workers=8, hbm_cap=40 << 30) as srv:
         rid = srv.submit_encode(data, Order.One)
         stream = srv.result(rid)            # bytes, or raises Malformed
         lat_us = srv.last_latency_us
 
 Requests are admitted in arrival order while their device-memory estimate fits
 under `hbm_cap`; a free worker codes every admitted request of the oldest
-request's kind and order mode as one batched pass.
+request's kind, order mode and size class (within a factor of four) as one
+batched pass.
 """
 
 from __future__ import annotations
@@ -39,7 +40,7 @@ def _lib():
 
 
 class Server:
-    def __init__(self, device: int = 0, workers: int = 4, hbm_cap: int = 40 << 30):
+    def __init__(self, device: int = 0, workers: int = 8, hbm_cap: int = 40 << 30):
         self._L = _lib()
         h = ctypes.c_void_p()
         rans.raise_for(self._L.fqxv_rans_server_create(device, workers, hbm_cap, ctypes.byref(h)))

@@ -179,10 +179,14 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
  * No reference counterpart. A server owns n_workers contexts (CUDA streams)
  * on one device. Requests (one stream each) are admitted in arrival order
  * while their device-memory estimate fits under hbm_cap (0: 40 GiB); a free
- * worker takes every admitted request with the oldest request's kind and
- * order mode and codes them as one batched pass, so requests arriving while
- * others run join the next pass and passes of different workers overlap on
- * the device. Results are byte-identical to the single calls. */
+ * worker takes every admitted request with the oldest request's kind, order
+ * mode and size class (input sizes within a factor of four) and codes them as
+ * one batched pass, so requests arriving while others run join the next pass
+ * and passes of different workers overlap on the device. Workers are warmed
+ * (pinned staging, one small pass per kernel path) before create returns.
+ * A decompress request whose declared length exceeds its max_len completes
+ * at submission with FQXV_RANS_E_BOUND. Results are byte-identical to the
+ * single calls. */
 typedef struct fqxv_rans_server fqxv_rans_server;
 
 int fqxv_rans_server_create(int device, int n_workers, uint64_t hbm_cap, fqxv_rans_server **out);

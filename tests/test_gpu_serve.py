@@ -97,3 +97,16 @@ def test_admission_cap_serialises_but_completes(gpu, orc):
             srv.submit_encode(bytes(64 << 20), rans.Order.One)   # larger than the cap
     for d, o in zip(data, outs):
         assert o == orc.encode(d, 1)
+
+
+def test_bound_is_checked_at_submission(gpu, orc):
+    rans, serve = gpu
+    data = W.binned_quality(50_000, 3).tobytes()
+    enc = orc.encode(data, 1)
+    with serve.Server(device=0, workers=2, hbm_cap=1 << 30) as srv:
+        bad = srv.submit_decode(enc, max_len=len(data) - 1)
+        good = srv.submit_decode(enc, max_len=len(data))
+        with pytest.raises(rans.Malformed) as e:
+            srv.result(bad)
+        assert e.value.status == 7
+        assert srv.result(good) == data
