@@ -23,6 +23,8 @@
 //      memory reads per round instead of 32).
 // Malformed input never faults: every read of the stream is bounds checked
 // and errors are reported per stream as the reference's Malformed kinds.
+#include <mutex>
+
 #include "rans_common.cuh"
 #include "rans_internal.cuh"
 
@@ -365,6 +367,8 @@ struct WordRing {
             __syncwarp();
         }
     }
+    // Byte `rel` (relative to the word region) from the ring.
+    __device__ __forceinline__ uint32_t byte(uint32_t rel) const { return ring[(lead + rel) & (kRingBytes - 1)]; }
     // Word j of the region; only the low bits of j matter (the ring is a
     // power-of-two window), so 32-bit arithmetic is exact here.
     __device__ __forceinline__ uint32_t word(uint32_t j) const {
@@ -513,10 +517,11 @@ __global__ void __launch_bounds__(32)
             uint8_t *op = out + r * 32 + lane;
 #pragma unroll
             for (int g = 0; g < G; g++) {
-                const uint32_t nW0 = R.word(w32 + lane);
-                const uint32_t nW1 = R.word(w32 + 32 + lane);
-                const uint32_t nPE0 = P[nW0 & (kTotFreq - 1)];
-                const uint32_t nPE1 = P[nW1 & (kTotFreq - 1)];
+                // The next window's bytes are loaded first and combined only
+                // after this round's shuffles, so no instruction of the
+                // state chain waits behind them (issue is in order).
+                const uint32_t b00 = R.byte(2 * (w32 + lane)), b01 = R.byte(2 * (w32 + lane) + 1);
+                const uint32_t b10 = R.byte(2 * (w32 + 32 + lane)), b11 = R.byte(2 * (w32 + 32 + lane) + 1);
                 const uint32_t v = ((e >> 20) + 1) * (x >> kScaleBits) + ((e >> 8) & 0xfffu);
                 const uint32_t ev = P[v & (kTotFreq - 1)];
                 const bool need = v < kRansL;
@@ -529,12 +534,12 @@ __global__ void __launch_bounds__(32)
                 op[32 * g] = (uint8_t)e;
                 x = need ? (v << 16) | w : v;
                 e = need ? pe : ev;
+                W0 = b00 | (b01 << 8);
+                W1 = b10 | (b11 << 8);
+                PE0 = P[W0 & (kTotFreq - 1)];
+                PE1 = P[W1 & (kTotFreq - 1)];
                 a = k;
                 w32 += k;
-                W0 = nW0;
-                W1 = nW1;
-                PE0 = nPE0;
-                PE1 = nPE1;
             }
             wp += (uint32_t)(w32 - (uint32_t)wp);
             r += G;
@@ -886,20 +891,41 @@ uint32_t dec_smem_bytes(int cls, int nd) {
     }
 }
 
+// Each decode kernel's dynamic shared-memory limit is raised once per
+// device to the largest size any launch uses. Setting it per launch would
+// race between host threads that launch the same kernel with different sizes
+// (a launch can find the limit lowered by another thread and fail).
+static std::mutex g_attr_mu;
+static bool g_attr_done[256];
+
+static void ensure_dec_attrs() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+        cudaGetLastError();
+        return;
+    }
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (g_attr_done[dev]) return;
+    cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dec_smem_bytes(kClsO0, 0));
+    cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dec_smem_bytes(kClsO1Dense, kDenseMax));
+    cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dec_smem_bytes(kClsO1Global, 0));
+    g_attr_done[dev] = true;
+}
+
 int dec_blocks_per_sm(int cls, uint32_t smem_bytes) {
+    ensure_dec_attrs();
     int n = 0;
     cudaError_t e = cudaSuccess;
     switch (cls) {
         case kClsO0:
-            cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o0_kernel, 32, smem_bytes);
             break;
         case kClsO1Dense:
-            cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1d_kernel, kO1Threads, smem_bytes);
             break;
         case kClsO1Global:
-            cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1g_kernel, 32, smem_bytes);
             break;
         default:
@@ -922,18 +948,16 @@ void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint3
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
                     cudaStream_t s) {
     if (nlist <= 0 || grid <= 0) return;
+    ensure_dec_attrs();
     switch (cls) {
         case kClsO0:
-            cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
             dec_o0_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
             break;
         case kClsO1Dense:
-            cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
             dec_o1d_kernel<<<grid, kO1Threads, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
                                                         smem_bytes - kO1Warps * kRingBytes);
             break;
         case kClsO1Global:
-            cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
             dec_o1g_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
             break;
         default:
