@@ -14,6 +14,8 @@
 //      and words written to their compacted place in the output arena.
 // Byte format and arithmetic follow crates/fqxv-rans/src/scalar.rs:29-140 and
 // model.rs:52-264.
+#include <mutex>
+
 #include "rans_common.cuh"
 #include "rans_internal.cuh"
 
@@ -217,7 +219,7 @@ __device__ __forceinline__ void enc_emit(bool need, uint32_t word, uint16_t *__r
 // warp vote per round) is kept off the state chain: a chunk records its
 // emit flags and pre-step states, and its words are written while the next
 // chunk's states are computed.
-template <int ORDER>
+template <int ORDER, bool SMEM_TAB>
 __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint64_t n,
                                             const uint2 *__restrict__ tab,
                                             const uint8_t *__restrict__ umap, uint32_t nu,
@@ -232,7 +234,8 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
     // Table entry of symbol s with predecessor `prev` (order-1: scalar.rs:85).
     auto entry = [&](uint32_t s, uint32_t prev) -> uint2 {
         if (ORDER == 0) return tab[s];
-        return __ldg(tab + (uint32_t)umap[prev] * nu + umap[s]);
+        const uint32_t idx = (uint32_t)umap[prev] * nu + umap[s];
+        return SMEM_TAB ? tab[idx] : __ldg(tab + idx);
     };
     if (rem) {
         const uint64_t i = (uint64_t)full * 32 + lane;
@@ -245,48 +248,56 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
         const bool need = enc_step(x, e, active);
         enc_emit(need, x_before, wptr, lt);
     }
-    uint32_t cur[16], nxt[16], wv[16], pwv[16];
+    // cur/nxt: symbols of this chunk and the next; for order-1 also the
+    // byte before each position (its context, scalar.rs:85; 0 before the
+    // first byte), loaded with them instead of exchanged between lanes.
+    uint32_t cur[16], nxt[16], curp[16], nxtp[16], wv[16], pwv[16];
     uint32_t pbits = 0;  // emit flags of the previous chunk (bit k = round rt + 16 - k)
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         const int64_t r = full - 1 - k;
-        cur[k] = r >= 0 ? (uint32_t)__ldg(p + (uint64_t)r * 32 + lane) : 0u;
+        const uint64_t i = (uint64_t)r * 32 + lane;
+        cur[k] = r >= 0 ? (uint32_t)__ldg(p + i) : 0u;
+        curp[k] = (ORDER == 1 && r >= 0 && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
         pwv[k] = 0;
     }
     for (int64_t rt = full - 1; rt >= 0; rt -= 16) {
-        if (rt >= 31) {
+        if (rt >= 32) {
             const uint8_t *pc = p + (uint64_t)(rt - 16) * 32 + lane;
 #pragma unroll
-            for (int k = 0; k < 16; k++) nxt[k] = (uint32_t)__ldg(pc - 32 * k);
+            for (int k = 0; k < 16; k++) {
+                nxt[k] = (uint32_t)__ldg(pc - 32 * k);
+                if (ORDER == 1) nxtp[k] = (uint32_t)__ldg(pc - 32 * k - 1);
+            }
         } else {
 #pragma unroll
             for (int k = 0; k < 16; k++) {
                 const int64_t r = rt - 16 - k;
-                nxt[k] = r >= 0 ? (uint32_t)__ldg(p + (uint64_t)r * 32 + lane) : 0u;
+                const uint64_t i = (uint64_t)r * 32 + lane;
+                nxt[k] = r >= 0 ? (uint32_t)__ldg(p + i) : 0u;
+                nxtp[k] = (ORDER == 1 && r >= 0 && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
             }
         }
         const bool whole = rt >= 15;
+        // The chunk's table entries first: they depend only on the symbols,
+        // so their loads overlap one another instead of stalling the state
+        // chain one round at a time (a warp issues in order).
+        uint2 ent[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) ent[k] = entry(cur[k], ORDER == 1 ? curp[k] : 0u);
         uint32_t bits = 0;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
-            uint32_t prev = 0;
-            if (ORDER == 1) {
-                // lane l > 0: lane l-1 of this round; lane 0: lane 31 of the
-                // round below (a guarded load gives 0 below round 0, which is
-                // the reference's initial context).
-                const uint32_t up = __shfl_up_sync(0xffffffffu, cur[k], 1);
-                const uint32_t p31 = __shfl_sync(0xffffffffu, k < 15 ? cur[k < 15 ? k + 1 : 15] : nxt[0], 31);
-                prev = lane ? up : p31;
-            }
             wv[k] = x;
             const bool active = whole || k <= rt;
-            if (enc_step(x, entry(cur[k], prev), active)) bits |= 1u << k;
+            if (enc_step(x, ent[k], active)) bits |= 1u << k;
             enc_emit((pbits >> k) & 1u, pwv[k], wptr, lt);
         }
         pbits = bits;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             cur[k] = nxt[k];
+            curp[k] = nxtp[k];
             pwv[k] = wv[k];
         }
     }
@@ -296,10 +307,16 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
     state = x;
 }
 
+// Order-1 tables of alphabets up to kEncO1SmemNu symbols are copied into
+// the warp's slice of dynamic shared memory; larger ones are read through L1.
+constexpr uint32_t kEncO1SmemNu = 45;
+constexpr uint32_t kEncO1TabBytes = (kEncO1SmemNu * kEncO1SmemNu * 8 + 127) / 128 * 128;
+
 __global__ void __launch_bounds__(kEncWarpsPerCta * 32)
     enc_run_kernel(const uint8_t *__restrict__ src, EncBlock *__restrict__ blocks,
                    const EncJob *__restrict__ jobs, int njobs, const uint8_t *__restrict__ tbl,
                    uint16_t *__restrict__ words, int *__restrict__ queue) {
+    extern __shared__ __align__(16) uint8_t dsm[];
     __shared__ uint2 s_tab[kEncWarpsPerCta][256];
     __shared__ uint8_t s_umap[kEncWarpsPerCta][256];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -322,13 +339,21 @@ __global__ void __launch_bounds__(kEncWarpsPerCta * 32)
 #pragma unroll
                 for (int k = 0; k < 8; k++) s_tab[warp][lane * 8 + k] = T0[lane * 8 + k];
                 __syncwarp();
-                encode_warp<0>(p, n, s_tab[warp], nullptr, 0, words, word_end, nw, st);
+                encode_warp<0, true>(p, n, s_tab[warp], nullptr, 0, words, word_end, nw, st);
             } else {
 #pragma unroll
                 for (int k = 0; k < 8; k++) s_umap[warp][lane * 8 + k] = T[kTblUmap + lane * 8 + k];
-                __syncwarp();
-                encode_warp<1>(p, n, reinterpret_cast<const uint2 *>(T + kTblO1), s_umap[warp],
-                               (uint32_t)B.nu, words, word_end, nw, st);
+                const uint32_t nu = (uint32_t)B.nu;
+                const uint2 *T1 = reinterpret_cast<const uint2 *>(T + kTblO1);
+                if (nu <= kEncO1SmemNu) {
+                    uint2 *t = reinterpret_cast<uint2 *>(dsm + warp * kEncO1TabBytes);
+                    for (uint32_t i = lane; i < nu * nu; i += 32) t[i] = T1[i];
+                    __syncwarp();
+                    encode_warp<1, true>(p, n, t, s_umap[warp], nu, words, word_end, nw, st);
+                } else {
+                    __syncwarp();
+                    encode_warp<1, false>(p, n, T1, s_umap[warp], nu, words, word_end, nw, st);
+                }
             }
         }
         B.states[job.order][lane] = st;
@@ -478,7 +503,22 @@ void launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *orde
 void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,
                     const uint8_t *tbl, uint16_t *words, int *queue, int grid, cudaStream_t s) {
     if (njobs <= 0) return;
-    enc_run_kernel<<<grid, kEncWarpsPerCta * 32, 0, s>>>(src, blocks, jobs, njobs, tbl, words, queue);
+    static std::mutex mu;
+    static bool done[256];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        // raised once per device: a per-launch setting would race between
+        // host threads (see the decode launchers)
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev >= 0 && dev < 256 && !done[dev]) {
+            cudaFuncSetAttribute(enc_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kEncWarpsPerCta * kEncO1TabBytes));
+            done[dev] = true;
+        }
+    }
+    enc_run_kernel<<<grid, kEncWarpsPerCta * 32, kEncWarpsPerCta * kEncO1TabBytes, s>>>(src, blocks, jobs, njobs,
+                                                                                       tbl, words, queue);
 }
 
 void launch_enc_select_scan(EncBlock *blocks, int nblocks, uint64_t *total, cudaStream_t s) {
