@@ -483,12 +483,13 @@ __global__ void __launch_bounds__(32)
         uint64_t wp = 0;
         int status = FQXV_RANS_OK;
         const uint64_t rounds = (n + 31) / 32, full = n / 32;
-        // Fast-path window: W0/W1 = words [wbase, wbase + 64) at lanes
-        // (lane, 32 + lane), PE0/PE1 = the table entries those words would
-        // select as the next slot, a = wp - wbase. A lane that renormalises
-        // takes word and next entry through one shuffle each, so the table
-        // lookup is off the round's critical path.
-        uint32_t W0 = 0, W1 = 0, PE0 = 0, PE1 = 0, a = 0, e = 0;
+        // Fast-path window: W = word wp + lane, PE = the table entry that
+        // word selects as the next slot. A lane that renormalises takes word
+        // and next entry through one shuffle each from lane popc(earlier
+        // needs), so the table lookup is off the round's critical path. The
+        // next window's bytes are loaded as soon as the round's vote is
+        // known and combined after its shuffles (a warp issues in order).
+        uint32_t W = 0, PE = 0, e = 0;
         bool window = false;
         uint64_t r = 0;
         if (rounds && !o0_general_round(x, P, 0, n, R, wp, navail, out, lt)) status = FQXV_RANS_E_TRUNCATED;
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(32)
         constexpr int G = 8;  // rounds per branch-free group
         while (status == FQXV_RANS_OK && r < rounds) {
             // A group of G full rounds takes at most 32 G words and its window
-            // reads 64 ahead, so it cannot run out of words or ring.
+            // reads 32 ahead, so it cannot run out of words or ring.
             if (r + G > full || wp + 32 * G + 64 > navail) {
                 if (!o0_general_round(x, P, r, n, R, wp, navail, out, lt)) status = FQXV_RANS_E_TRUNCATED;
                 r++;
@@ -506,40 +507,28 @@ __global__ void __launch_bounds__(32)
             R.advance(wp);
             uint32_t w32 = (uint32_t)wp;
             if (!window) {
-                W0 = R.word(w32 + lane);
-                W1 = R.word(w32 + 32 + lane);
-                PE0 = P[W0 & (kTotFreq - 1)];
-                PE1 = P[W1 & (kTotFreq - 1)];
-                a = 0;
+                W = R.word(w32 + lane);
+                PE = P[W & (kTotFreq - 1)];
                 e = P[x & (kTotFreq - 1)];
                 window = true;
             }
             uint8_t *op = out + r * 32 + lane;
 #pragma unroll
             for (int g = 0; g < G; g++) {
-                // The next window's bytes are loaded first and combined only
-                // after this round's shuffles, so no instruction of the
-                // state chain waits behind them (issue is in order).
-                const uint32_t b00 = R.byte(2 * (w32 + lane)), b01 = R.byte(2 * (w32 + lane) + 1);
-                const uint32_t b10 = R.byte(2 * (w32 + 32 + lane)), b11 = R.byte(2 * (w32 + 32 + lane) + 1);
                 const uint32_t v = ((e >> 20) + 1) * (x >> kScaleBits) + ((e >> 8) & 0xfffu);
                 const uint32_t ev = P[v & (kTotFreq - 1)];
                 const bool need = v < kRansL;
                 const uint32_t mask = __ballot_sync(0xffffffffu, need);
-                const uint32_t k = __popc(mask);
-                const uint32_t srcl = (a + __popc(mask & lt)) & 31u;
-                const bool lo = (uint32_t)lane >= a;
-                const uint32_t w = __shfl_sync(0xffffffffu, lo ? W0 : W1, srcl);
-                const uint32_t pe = __shfl_sync(0xffffffffu, lo ? PE0 : PE1, srcl);
+                const uint32_t srcl = __popc(mask & lt);
+                w32 += __popc(mask);
+                const uint32_t b0 = R.byte(2 * (w32 + lane)), b1 = R.byte(2 * (w32 + lane) + 1);
+                const uint32_t w = __shfl_sync(0xffffffffu, W, srcl);
+                const uint32_t pe = __shfl_sync(0xffffffffu, PE, srcl);
                 op[32 * g] = (uint8_t)e;
                 x = need ? (v << 16) | w : v;
                 e = need ? pe : ev;
-                W0 = b00 | (b01 << 8);
-                W1 = b10 | (b11 << 8);
-                PE0 = P[W0 & (kTotFreq - 1)];
-                PE1 = P[W1 & (kTotFreq - 1)];
-                a = k;
-                w32 += k;
+                W = b0 | (b1 << 8);
+                PE = P[W & (kTotFreq - 1)];
             }
             wp += (uint32_t)(w32 - (uint32_t)wp);
             r += G;
