@@ -311,12 +311,13 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     }
     if (persistent) {
         cudaEvent_t t0 = ctx->timer.begin(s);
-        launch_enc_pack(dB, (int)nb, dT, dW, d_dst, (int)std::min<size_t>(nb, (size_t)ctx->sms * 8), s);
+        launch_enc_pack(dB, (int)nb, dT, dW, d_dst, (int)std::min<size_t>(nb * kPackParts, (size_t)ctx->sms * 8),
+                        s);
         ctx->timer.end(kStEncPack, t0, s);
     } else {
         for (size_t j = 0; j < nb; j++) {
             cudaEvent_t t0 = ctx->timer.begin(s);
-            launch_enc_pack(dB + j, 1, dT, dW, d_dst, 1, s);
+            launch_enc_pack(dB + j, 1, dT, dW, d_dst, kPackParts, s);
             ctx->timer.end(kStEncPack, t0, s);
         }
     }

@@ -409,6 +409,33 @@ __global__ void __launch_bounds__(1024)
     if (tid == 0) *total = carry;
 }
 
+// Bytes [lo, hi) of src to the same positions of dst, by the whole CTA:
+// 4-byte stores at aligned destination addresses, each assembled from the
+// two aligned source words it straddles (a load never leaves the aligned
+// word of a byte it needs).
+__device__ __forceinline__ void cta_copy(uint8_t *__restrict__ dst, const uint8_t *__restrict__ src, uint64_t lo,
+                                         uint64_t hi) {
+    const uint32_t tid = threadIdx.x;
+    if (hi <= lo) return;
+    const uint64_t lead = (4u - ((uintptr_t)(dst + lo) & 3u)) & 3u;
+    const uint64_t head = lead < hi - lo ? lead : hi - lo;
+    if (tid < head) dst[lo + tid] = src[lo + tid];
+    const uint64_t a = lo + head;
+    const uint64_t nw = (hi - a) / 4;
+    const uint32_t sh = (uint32_t)((uintptr_t)(src + a) & 3u);
+    const uint32_t *s4 = reinterpret_cast<const uint32_t *>((uintptr_t)(src + a) & ~(uintptr_t)3);
+    uint32_t *d4 = reinterpret_cast<uint32_t *>(dst + a);
+    if (sh == 0) {
+        for (uint64_t j = tid; j < nw; j += blockDim.x) d4[j] = s4[j];
+    } else {
+        for (uint64_t j = tid; j < nw; j += blockDim.x) d4[j] = __funnelshift_r(s4[j], s4[j + 1], 8 * sh);
+    }
+    const uint64_t t = a + 4 * nw;
+    if (tid < hi - t) dst[t + tid] = src[t + tid];
+}
+
+// One work item per (block, part): part 0 writes the header, tables and
+// states, and every part copies its slice of the renorm words.
 __global__ void __launch_bounds__(kPackThreads)
     enc_pack_kernel(const EncBlock *__restrict__ blocks, int nblocks, const uint8_t *__restrict__ tbl,
                     const uint16_t *__restrict__ words, uint8_t *__restrict__ dst) {
@@ -416,11 +443,23 @@ __global__ void __launch_bounds__(kPackThreads)
     __shared__ uint8_t rowctx[256];
     __shared__ int s_k;
     const int tid = threadIdx.x;
-    for (int b = blockIdx.x; b < nblocks; b += gridDim.x) {
+    const int nitems = nblocks * kPackParts;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int b = item / kPackParts, part = item % kPackParts;
         const EncBlock &B = blocks[b];
         const int o = B.chosen;
         const uint64_t n = B.n;
         uint8_t *d = dst + B.out_off;
+        if (n == 0 && part != 0) continue;
+        const uint64_t hdr = o == 0 ? kHdr + kO0Tables : kHdr + kO1Bitmap + kO1Table * (uint64_t)B.nctx;
+        if (part != 0) {
+            const uint64_t W2 = 2 * B.nwords[o];
+            const uint64_t lo = (W2 * part / kPackParts) & ~(uint64_t)15;
+            const uint64_t hi = part + 1 == kPackParts ? W2 : (W2 * (part + 1) / kPackParts) & ~(uint64_t)15;
+            const uint8_t *ws = reinterpret_cast<const uint8_t *>(words + B.word_off[o] + n - B.nwords[o]);
+            cta_copy(d + hdr + kStatesBytes, ws, lo, hi);
+            continue;
+        }
         if (tid == 0) d[0] = (uint8_t)o;
         if (tid >= 1 && tid <= 8) d[tid] = (uint8_t)(n >> (8 * (tid - 1)));
         if (n == 0) continue;
@@ -483,13 +522,9 @@ __global__ void __launch_bounds__(kPackThreads)
             for (int k = 0; k < 4; k++) d[off + 4 * tid + k] = (uint8_t)(x >> (8 * k));
         }
         off += kStatesBytes;
-        const uint64_t W = B.nwords[o];
-        const uint16_t *ws = words + B.word_off[o] + n - W;
-        for (uint64_t j = tid; j < W; j += blockDim.x) {
-            const uint16_t w = ws[j];
-            d[off + 2 * j] = (uint8_t)w;
-            d[off + 2 * j + 1] = (uint8_t)(w >> 8);
-        }
+        const uint64_t W2 = 2 * B.nwords[o];
+        const uint8_t *ws = reinterpret_cast<const uint8_t *>(words + B.word_off[o] + n - B.nwords[o]);
+        cta_copy(d + off, ws, 0, kPackParts == 1 ? W2 : (W2 / kPackParts) & ~(uint64_t)15);
         __syncthreads();
     }
 }

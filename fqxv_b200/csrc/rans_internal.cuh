@@ -28,6 +28,7 @@ constexpr int kEncWarpsPerCta = 4;          // encode: one warp per (block, orde
 constexpr int kDecWarpsPerCta = 4;          // decode: one warp per stream
 constexpr int kParseThreads = 256;          // decode header/table kernel
 constexpr int kPackThreads = 256;           // output compaction
+constexpr int kPackParts = 8;               // output compaction: CTAs per block
 
 // Encode-side descriptor of one input block (device resident).
 struct EncBlock {
