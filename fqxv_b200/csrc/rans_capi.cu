@@ -246,7 +246,8 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         if (o1) jobs.push_back({b, 1});
         if (o0) jobs.push_back({b, 0});
     }
-    const int model_grid = (int)std::min<size_t>(nb, (size_t)ctx->sms * 2);
+    // clusters of the model kernel: as many as are resident at once
+    const int model_grid = (int)std::min<size_t>(nb, std::max<size_t>(1, (size_t)ctx->sms * 4 / kModelCluster));
     CK(ctx->e_blocks.ensure(nb * sizeof(EncBlock), s));
     CK(ctx->e_order.ensure(nb * sizeof(uint32_t), s));
     CK(ctx->e_jobs.ensure(jobs.size() * sizeof(EncJob), s));
@@ -278,7 +279,7 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     const int run_grid = ctx->sms * 16;
     if (persistent) {
         cudaEvent_t t0 = ctx->timer.begin(s);
-        launch_enc_model(d_src, dB, dO, (int)nb, dT, dH, model_grid, s);
+        CK(launch_enc_model(d_src, dB, dO, (int)nb, dT, dH, model_grid, s));
         ctx->timer.end(kStEncModel, t0, s);
         t0 = ctx->timer.begin(s);
         launch_enc_run(d_src, dB, dJ, (int)jobs.size(), dT, dW, queue,
@@ -290,7 +291,7 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         for (size_t j = 0; j < nb; j++) {
             CK(cudaMemsetAsync(queue, 0, 4, s));
             cudaEvent_t t0 = ctx->timer.begin(s);
-            launch_enc_model(d_src, dB, dO + j, 1, dT, dH, 1, s);
+            CK(launch_enc_model(d_src, dB, dO + j, 1, dT, dH, 1, s));
             ctx->timer.end(kStEncModel, t0, s);
             t0 = ctx->timer.begin(s);
             launch_enc_run(d_src, dB, dJ + j * per, per, dT, dW, queue, 1, s);

@@ -14,6 +14,7 @@
 //      and words written to their compacted place in the output arena.
 // Byte format and arithmetic follow crates/fqxv-rans/src/scalar.rs:29-140 and
 // model.rs:52-264.
+#include <cooperative_groups.h>
 #include <mutex>
 
 #include "rans_common.cuh"
@@ -29,23 +30,24 @@ __device__ __forceinline__ void unpack16(const uint4 v, uint32_t b[16]) {
     for (int k = 0; k < 16; k++) b[k] = (w[k >> 2] >> (8 * (k & 3))) & 0xffu;
 }
 
-// Visit p[0, n) in 16-byte aligned vector chunks (one per thread per step) and
-// in single bytes for the unaligned head and the tail. For every byte the
-// visitor gets (previous byte or 0 at position 0, byte); `flush` folds runs of
-// equal keys into one shared-memory atomic.
+// Visit positions [lo, hi) of the block p in 16-byte aligned vector chunks
+// (one per thread per step) and in single bytes for the unaligned head and
+// the tail. For every byte the visitor gets (previous byte or 0 at position
+// 0, byte); runs of equal keys are folded into one shared-memory atomic.
 template <class KeyFn, class AddFn>
-__device__ __forceinline__ void histogram_pass(const uint8_t *__restrict__ p, uint64_t n, KeyFn key,
+__device__ __forceinline__ void histogram_pass(const uint8_t *__restrict__ p, uint64_t lo, uint64_t hi, KeyFn key,
                                                AddFn add) {
-    const uint64_t mis = (uint64_t)(uintptr_t)p & 15u;
+    if (hi <= lo) return;
+    const uint64_t n = hi - lo;
+    const uint64_t mis = (uint64_t)(uintptr_t)(p + lo) & 15u;
     uint64_t head = mis ? 16 - mis : 0;
     if (head > n) head = n;
     const uint64_t body = (n - head) / 16;
-    const uint64_t tail0 = head + body * 16;
-    for (uint64_t i = threadIdx.x; i < head; i += blockDim.x) add(key(i ? p[i - 1] : 0u, p[i]), 1u);
-    for (uint64_t i = tail0 + threadIdx.x; i < n; i += blockDim.x)
-        add(key(i ? p[i - 1] : 0u, p[i]), 1u);
+    const uint64_t tail0 = lo + head + body * 16;
+    for (uint64_t i = lo + threadIdx.x; i < lo + head; i += blockDim.x) add(key(i ? p[i - 1] : 0u, p[i]), 1u);
+    for (uint64_t i = tail0 + threadIdx.x; i < hi; i += blockDim.x) add(key(i ? p[i - 1] : 0u, p[i]), 1u);
     for (uint64_t c = threadIdx.x; c < body; c += blockDim.x) {
-        const uint64_t pos = head + 16 * c;
+        const uint64_t pos = lo + head + 16 * c;
         const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p + pos));
         uint32_t b[16];
         unpack16(v, b);
@@ -77,45 +79,61 @@ __device__ __forceinline__ uint2 enc_entry(uint32_t f, uint32_t cum) {
 
 }  // namespace
 
+// Model of one block per thread-block cluster of kModelCluster CTAs: every
+// CTA histograms its slice of the block into its own shared memory and the
+// slices are summed through distributed shared memory. Counts: scalar.rs:30-33
+// (order-0) and :62-80 (order-1); normalisation: model.rs:213-264.
 __global__ void __launch_bounds__(kModelThreads)
     enc_model_kernel(const uint8_t *__restrict__ src, EncBlock *__restrict__ blocks,
                      const uint32_t *__restrict__ order, int nblocks, uint8_t *__restrict__ tbl,
                      uint32_t *__restrict__ hist_scratch) {
+    namespace cg = cooperative_groups;
     constexpr int W = kModelThreads / 32;
     constexpr int kSmemU = 64;
     __shared__ uint32_t h0[W][256];
     __shared__ uint32_t h1[kSmemU * kSmemU];
-    __shared__ uint32_t cnt[256];
+    __shared__ uint32_t part[256];      // this CTA's order-0 counts
+    __shared__ uint32_t cnt[256];       // the block's order-0 counts
+    __shared__ uint32_t rowbuf[W][kSmemU];
     __shared__ uint8_t umap[256];
     __shared__ int s_nu, s_nctx;
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    uint32_t *gh = hist_scratch + (size_t)blockIdx.x * 65536;
+    const int cid = blockIdx.x / C, ncl = gridDim.x / C;
+    uint32_t *gh = hist_scratch + (size_t)cid * 65536;
 
-    for (int bi = blockIdx.x; bi < nblocks; bi += gridDim.x) {
+    for (int bi = cid; bi < nblocks; bi += ncl) {
         const int b = order[bi];
         const uint8_t *p = src + blocks[b].src_off;
         const uint64_t n = blocks[b].n;
         const int mode = blocks[b].mode;
         uint8_t *T = tbl + blocks[b].tbl_off;
+        const uint64_t lo = n * (uint64_t)rank / C, hi = n * (uint64_t)(rank + 1) / C;
 
         for (int i = tid; i < W * 256; i += blockDim.x) (&h0[0][0])[i] = 0;
         if (tid == 0) s_nctx = 0;
         __syncthreads();
-        // Pass A: order-0 counts (scalar.rs:30-33).
         uint32_t *hw = h0[warp];
         histogram_pass(
-            p, n, [](uint32_t, uint32_t c) { return c; },
+            p, lo, hi, [](uint32_t, uint32_t c) { return c; },
             [&](uint32_t k, uint32_t r) { atomicAdd(&hw[k], r); });
         __syncthreads();
         if (tid < 256) {
-            uint32_t s = 0;
+            uint32_t t = 0;
 #pragma unroll
-            for (int w = 0; w < W; w++) s += h0[w][tid];
-            cnt[tid] = s;
+            for (int w = 0; w < W; w++) t += h0[w][tid];
+            part[tid] = t;
+        }
+        cl.sync();  // every slice's counts are in place
+        if (tid < 256) {
+            uint32_t t = 0;
+            for (int r = 0; r < C; r++) t += cl.map_shared_rank(part, r)[tid];
+            cnt[tid] = t;
         }
         __syncthreads();
 
-        if (mode != FQXV_RANS_ORDER1 && warp == 0) {
+        if (mode != FQXV_RANS_ORDER1 && rank == 0 && warp == 0) {
             uint32_t f[8], cum[8];
             bool present;
             warp_normalize(cnt, 256, f, cum, present);
@@ -124,12 +142,13 @@ __global__ void __launch_bounds__(kModelThreads)
             for (int k = 0; k < 8; k++) T0[lane * 8 + k] = enc_entry(f[k], cum[k]);
         }
         if (mode == FQXV_RANS_ORDER0) {
-            __syncthreads();
+            cl.sync();  // no CTA rewrites `part` while another still reads it
             continue;
         }
 
         // Order-1 (scalar.rs:62-80). U = occurring bytes plus context 0, in
         // ascending byte order; contexts and symbols share that dense index.
+        // Every CTA derives the same map from the same counts.
         if (warp == 0) {
             uint32_t flags = 0;
 #pragma unroll
@@ -148,33 +167,61 @@ __global__ void __launch_bounds__(kModelThreads)
         }
         __syncthreads();
         const int nu = s_nu;
-        const bool in_smem = nu <= kSmemU;
-        uint32_t *H = in_smem ? h1 : gh;
-        for (int i = tid; i < nu * nu; i += blockDim.x) H[i] = 0;
-        if (tid < 256) T[kTblUmap + tid] = umap[tid];
-        __syncthreads();
-        histogram_pass(
-            p, n, [&](uint32_t prev, uint32_t c) { return (uint32_t)umap[prev] * nu + umap[c]; },
-            [&](uint32_t k, uint32_t r) { atomicAdd(&H[k], r); });
-        __syncthreads();
+        auto pair = [&](uint32_t prev, uint32_t c) { return (uint32_t)umap[prev] * nu + umap[c]; };
         uint2 *T1 = reinterpret_cast<uint2 *>(T + kTblO1);
-        for (int t = warp; t < nu; t += W) {
-            uint32_t f[8], cum[8];
-            bool present;
-            warp_normalize(H + (size_t)t * nu, nu, f, cum, present);
+        if (rank == 0 && tid < 256) T[kTblUmap + tid] = umap[tid];
+        if (nu <= kSmemU) {
+            // pair counts of this slice in shared memory, rows summed over
+            // the cluster; context rows are spread over all warps of it
+            for (int i = tid; i < nu * nu; i += blockDim.x) h1[i] = 0;
+            __syncthreads();
+            histogram_pass(p, lo, hi, pair, [&](uint32_t k, uint32_t r) { atomicAdd(&h1[k], r); });
+            cl.sync();
+            for (int t = warp + W * rank; t < nu; t += W * C) {
+                for (int u = lane; u < nu; u += 32) {
+                    uint32_t v = 0;
+                    for (int r = 0; r < C; r++) v += cl.map_shared_rank(h1, r)[t * nu + u];
+                    rowbuf[warp][u] = v;
+                }
+                __syncwarp();
+                uint32_t f[8], cum[8];
+                bool present;
+                warp_normalize(rowbuf[warp], nu, f, cum, present);
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const int u = lane * 8 + k;
-                if (u < nu) T1[(size_t)t * nu + u] = enc_entry(f[k], cum[k]);
+                for (int k = 0; k < 8; k++) {
+                    const int u = lane * 8 + k;
+                    if (u < nu) T1[(size_t)t * nu + u] = enc_entry(f[k], cum[k]);
+                }
+                if (lane == 0 && present) atomicAdd(&s_nctx, 1);
+                __syncwarp();
             }
-            if (lane == 0 && present) atomicAdd(&s_nctx, 1);
+        } else if (rank == 0) {
+            // large alphabets: the cluster's first CTA counts the whole block
+            // in global scratch
+            for (int i = tid; i < nu * nu; i += blockDim.x) gh[i] = 0;
+            __syncthreads();
+            histogram_pass(p, 0, n, pair, [&](uint32_t k, uint32_t r) { atomicAdd(&gh[k], r); });
+            __syncthreads();
+            for (int t = warp; t < nu; t += W) {
+                uint32_t f[8], cum[8];
+                bool present;
+                warp_normalize(gh + (size_t)t * nu, nu, f, cum, present);
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int u = lane * 8 + k;
+                    if (u < nu) T1[(size_t)t * nu + u] = enc_entry(f[k], cum[k]);
+                }
+                if (lane == 0 && present) atomicAdd(&s_nctx, 1);
+            }
         }
-        __syncthreads();
-        if (tid == 0) {
+        cl.sync();  // all rows done; s_nctx final in every CTA
+        if (rank == 0 && tid == 0) {
+            int k = 0;
+            for (int r = 0; r < C; r++) k += *cl.map_shared_rank(&s_nctx, r);
             blocks[b].nu = nu;
-            blocks[b].nctx = s_nctx;
+            blocks[b].nctx = k;
         }
-        __syncthreads();
+        cl.sync();  // no CTA rewrites shared state while another still reads it
     }
 }
 
@@ -529,10 +576,23 @@ __global__ void __launch_bounds__(kPackThreads)
     }
 }
 
-void launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
-                      uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s) {
-    if (nblocks <= 0) return;
-    enc_model_kernel<<<grid, kModelThreads, 0, s>>>(src, blocks, order, nblocks, tbl, hist_scratch);
+cudaError_t launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
+                             uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s) {
+    if (nblocks <= 0) return cudaSuccess;
+    // `grid` clusters of kModelCluster CTAs
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid * kModelCluster, 1, 1);
+    cfg.blockDim = dim3(kModelThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kModelCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, enc_model_kernel, src, blocks, order, nblocks, tbl, hist_scratch);
 }
 
 void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,

@@ -23,7 +23,8 @@ constexpr uint64_t kO1Table = 512;          // 256 x u16 per present context
 constexpr uint64_t kStatesBytes = 4 * kStates;
 
 // Persistent-kernel shapes.
-constexpr int kModelThreads = 512;          // model kernel: one CTA per block
+constexpr int kModelThreads = 512;          // model kernel: threads per CTA
+constexpr int kModelCluster = 8;            // model kernel: CTAs (one cluster) per block
 constexpr int kEncWarpsPerCta = 4;          // encode: one warp per (block, order)
 constexpr int kDecWarpsPerCta = 4;          // decode: one warp per stream
 constexpr int kParseThreads = 256;          // decode header/table kernel
@@ -136,8 +137,9 @@ constexpr uint32_t kOutRows = 3 * kDenseMax + 1;
 inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 // ---- launchers (rans_encode.cu / rans_decode.cu) ---------------------------
-void launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
-                      uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s);
+// `grid` clusters of kModelCluster CTAs; returns the launch status.
+cudaError_t launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
+                             uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s);
 void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,
                     const uint8_t *tbl, uint16_t *words, int *queue, int grid, cudaStream_t s);
 void launch_enc_select_scan(EncBlock *blocks, int nblocks, uint64_t *total, cudaStream_t s);
