@@ -44,7 +44,9 @@ __global__ void __launch_bounds__(kParseThreads)
     __shared__ uint8_t ctxlist[256];  // present-table index -> raw context
     __shared__ uint8_t dmap[256];     // raw byte -> dense index (0xFF not in D)
     __shared__ uint8_t symseen[256];
-    __shared__ int s_k, s_nd;
+    __shared__ __align__(16) uint8_t smap[kParseThreads / 32][kTotFreq];  // per warp: slot -> dense symbol
+    __shared__ int s_k, s_nd, s_bad;
+    __shared__ uint8_t s_badst[256];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     for (int si = blockIdx.x; si < nstreams; si += gridDim.x) {
@@ -144,21 +146,37 @@ __global__ void __launch_bounds__(kParseThreads)
                 if (lane == 31) s_k = (int)base;
             }
             if (tid < 256) symseen[tid] = 0;
+            if (tid == 0) s_bad = 1 << 30;
             __syncthreads();
             const int K = s_k;
-            // Pass 1: every table in ascending context order -- truncation and
-            // validity are reported for the first failing table (scalar.rs:186-194).
-            for (int t = 0; t < K; t++) {
+            // Pass 1: every table checked, one warp per table; the first
+            // failing table in ascending context order decides the error,
+            // truncation or validity, as the reference's sequential reads
+            // do (scalar.rs:186-194, model.rs:160-174).
+            for (int t = warp; t < K; t += kParseThreads / 32) {
                 const uint64_t at = kHdr + kO1Bitmap + kO1Table * (uint64_t)t;
+                int st = FQXV_RANS_OK;
                 if (L < at + kO1Table) {
-                    status = FQXV_RANS_E_TRUNCATED;
-                    break;
+                    st = FQXV_RANS_E_TRUNCATED;
+                } else {
+                    uint32_t tot = 0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const uint32_t f = (uint32_t)p[at + 16 * lane + 2 * k] | ((uint32_t)p[at + 16 * lane + 2 * k + 1] << 8);
+                        tot += f;
+                        if (f) symseen[lane * 8 + k] = 1;
+                    }
+                    const uint64_t tt = warp_sum_u64(tot);
+                    // running sums are monotone: "some prefix exceeds" == "total exceeds"
+                    st = tt > kTotFreq ? FQXV_RANS_E_FREQ_EXCEEDS : (tt != kTotFreq ? FQXV_RANS_E_FREQ_SUM : FQXV_RANS_OK);
                 }
-                status = load_table(at);
-                if (status != FQXV_RANS_OK) break;
-                if (tid < 256 && sfreq[tid]) symseen[tid] = 1;
-                __syncthreads();
+                if (st != FQXV_RANS_OK && lane == 0) {
+                    s_badst[t] = (uint8_t)st;
+                    atomicMin(&s_bad, t);
+                }
             }
+            __syncthreads();
+            if (s_bad < K) status = s_badst[s_bad];
             hdr = kHdr + kO1Bitmap + kO1Table * (uint64_t)K;
             if (status == FQXV_RANS_OK && L < hdr + kStatesBytes) status = FQXV_RANS_E_TRUNCATED;
             if (status == FQXV_RANS_OK && n > S.dst_cap) status = FQXV_RANS_E_ALLOC;
@@ -202,17 +220,47 @@ __global__ void __launch_bounds__(kParseThreads)
                     for (int i = tid; i < stride * stride; i += blockDim.x) FC[i] = 0;
                     if (tid < 256 && dmap[tid] != 0xff) DS[dmap[tid]] = (uint8_t)tid;
                     __syncthreads();
-                    // Pass 2: chain rows and FC rows of the present contexts.
-                    for (int t = 0; t < K; t++) {
-                        load_table(kHdr + kO1Bitmap + kO1Table * (uint64_t)t);
+                    // Pass 2: chain rows and FC rows of the present contexts,
+                    // one warp per context: the warp paints each symbol's slot
+                    // range [cum, cum + f) into its shared slot map, then
+                    // stores the map as the context's chain row.
+                    uint8_t *sm = smap[warp];
+                    for (int t = warp; t < K; t += kParseThreads / 32) {
+                        const uint64_t at = kHdr + kO1Bitmap + kO1Table * (uint64_t)t;
                         const int dc = dmap[ctxlist[t]];
-                        uint8_t *row = CT + (uint64_t)dc * kChainStride;
-                        for (int slot = tid; slot < (int)kTotFreq; slot += blockDim.x)
-                            row[slot] = dmap[slot_sym((uint32_t)slot)];
-                        if (tid < 256 && sfreq[tid])
-                            FC[dc * stride + dmap[tid]] = (sfreq[tid] << kScaleBits) | scum[tid];
-                        __syncthreads();
+                        uint32_t f[8], cum[8], run = 0;
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            f[k] = (uint32_t)p[at + 16 * lane + 2 * k] | ((uint32_t)p[at + 16 * lane + 2 * k + 1] << 8);
+                            cum[k] = run;
+                            run += f[k];
+                        }
+                        const uint32_t base = warp_incl_scan(run) - run;
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            cum[k] += base;
+                            const uint32_t sym = lane * 8 + k;
+                            if (f[k]) FC[dc * stride + dmap[sym]] = (f[k] << kScaleBits) | cum[k];
+                        }
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            uint32_t m = __ballot_sync(0xffffffffu, f[k] != 0);
+                            while (m) {
+                                const int src = __ffs(m) - 1;
+                                m &= m - 1;
+                                const uint32_t c0 = __shfl_sync(0xffffffffu, cum[k], src);
+                                const uint32_t fk = __shfl_sync(0xffffffffu, f[k], src);
+                                const uint8_t dv = dmap[src * 8 + k];
+                                for (uint32_t i = lane; i < fk; i += 32) sm[c0 + i] = dv;
+                            }
+                        }
+                        __syncwarp();
+                        uint32_t *row = reinterpret_cast<uint32_t *>(CT + (uint64_t)dc * kChainStride);
+                        const uint32_t *sm32 = reinterpret_cast<const uint32_t *>(sm);
+                        for (int i = lane; i < (int)kTotFreq / 4; i += 32) row[i] = sm32[i];
+                        __syncwarp();
                     }
+                    __syncthreads();
                     if (tid == 0) {
                         S.cls = kClsO1Dense;
                         S.nd = nd;
