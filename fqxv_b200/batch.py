@@ -112,7 +112,7 @@ class Codec:
         return out, orders
 
     def decode_batch_host(self, h_src: np.ndarray, spans, out_spans, h_dst: np.ndarray,
-                          max_len: int | None = None):
+                          max_len: int | None = None, raise_on_error: bool = True):
         s = _spans(spans)
         o = _spans(out_spans)
         nb = len(s)
@@ -122,7 +122,8 @@ class Codec:
         st = self._lib.fqxv_rans_decode_batch_host(self._h, h_src.ctypes.data, s.ctypes.data, nb, ml,
                                                    h_dst.ctypes.data, o.ctypes.data, lens.ctypes.data,
                                                    status.ctypes.data)
-        rans.raise_for(st)
+        if st and (raise_on_error or st not in rans.MALFORMED):
+            rans.raise_for(st)
         return lens, status
 
     # ---- per-stage timing ---------------------------------------------------

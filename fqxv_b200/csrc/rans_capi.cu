@@ -210,6 +210,18 @@ uint64_t enc_bound_one(uint64_t n, int order) {
     return kHdr + tables + kStatesBytes + 2 * n;
 }
 
+// Device address of a pinned, mapped host buffer (nullptr for any other
+// memory): with unified addressing a kernel can load and store it directly.
+void *mapped_device_ptr(const void *h) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost) return nullptr;
+    return a.devicePointer;
+}
+
 int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks,
                       size_t nb, int mode, uint8_t *d_dst, uint64_t dst_cap, fqxv_rans_span *out_spans,
                       int32_t *out_orders, int persistent) {
@@ -750,15 +762,34 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
         end = std::max<uint64_t>(end, blocks[i].offset + blocks[i].length);
         oend = std::max<uint64_t>(oend, out_spans[i].offset + out_spans[i].length);
     }
-    CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
-    CK(ctx->io_out.ensure(std::max<uint64_t>(oend, 16), s));
-    CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
+    // Pinned (mapped) host buffers are read and written by the kernels in
+    // place over the host link, so the transfers overlap the decode instead
+    // of preceding and following it; other buffers are staged by copies.
+    const uint8_t *d_in = static_cast<const uint8_t *>(mapped_device_ptr(h_src));
+    uint8_t *d_out = static_cast<uint8_t *>(mapped_device_ptr(h_dst));
+    if (!d_in) {
+        CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
+        CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
+        d_in = ctx->io_in.as<uint8_t>();
+    }
+    const bool staged_out = d_out == nullptr;
+    if (staged_out) {
+        CK(ctx->io_out.ensure(std::max<uint64_t>(oend, 16), s));
+        d_out = ctx->io_out.as<uint8_t>();
+    }
     std::vector<uint64_t> lens(nblocks);
     std::vector<int32_t> sts(nblocks);
-    const int first = decode_batch_impl(ctx, ctx->io_in.as<uint8_t>(), blocks, nblocks, max_len,
-                                        ctx->io_out.as<uint8_t>(), out_spans, lens.data(), sts.data(), 1);
+    const int first = decode_batch_impl(ctx, d_in, blocks, nblocks, max_len, d_out, out_spans, lens.data(),
+                                        sts.data(), 1);
     if (first != FQXV_RANS_OK && (first < FQXV_RANS_E_TRUNCATED || first > FQXV_RANS_E_TRUNCATED_RENORM))
         return first;
+    if (!staged_out) {
+        for (size_t i = 0; i < nblocks; i++) {
+            if (out_lens) out_lens[i] = lens[i];
+            if (status) status[i] = sts[i];
+        }
+        return first;
+    }
     // One copy of the whole output range when the spans are dense, else one
     // copy per decoded block.
     uint64_t produced = 0;

@@ -140,3 +140,36 @@ def test_decode_batch_per_block_status(codec, orc):
         assert st[i] == ws, i
         if ws == 0:
             assert dec[int(doffs[i]):int(doffs[i]) + int(olens[i])].tobytes() == wb
+
+
+def test_host_decode_pinned_and_pageable_agree(codec, orc):
+    """Pinned buffers are decoded in place by the kernels, pageable ones
+    through staging copies; both give the oracle's bytes and statuses."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    streams, want = [], []
+    for i in range(24):
+        blk = W.GENERATORS[list(W.GENERATORS)[i % 4]](int(rng.integers(1, 200_000)), 40 + i).tobytes()
+        e = bytearray(orc.encode(blk, i % 2))
+        if i % 7 == 3:
+            e = e[:len(e) // 2]      # truncated
+        streams.append(bytes(e))
+        want.append(orc.decode_status(bytes(e), max_len=1 << 18))
+    lens = np.array([len(s) for s in streams], np.uint64)
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint64)
+    arena = np.frombuffer(b"".join(streams), np.uint8)
+    caps = np.full(len(streams), 1 << 18, np.uint64)
+    doffs = np.arange(len(streams), dtype=np.uint64) << np.uint64(18)
+    spans, ospans = np.stack([offs, lens], 1), np.stack([doffs, caps], 1)
+    pin_src = torch.from_numpy(arena.copy()).pin_memory().numpy()
+    pin_dst = torch.zeros(len(streams) << 18, dtype=torch.uint8).pin_memory().numpy()
+    page_dst = np.zeros(len(streams) << 18, np.uint8)
+    l1, s1 = codec.decode_batch_host(pin_src, spans, ospans, pin_dst, max_len=1 << 18, raise_on_error=False)
+    l2, s2 = codec.decode_batch_host(arena.copy(), spans, ospans, page_dst, max_len=1 << 18, raise_on_error=False)
+    for i, (ws, wb) in enumerate(want):
+        assert s1[i] == ws and s2[i] == ws, i
+        if ws == 0:
+            o = int(doffs[i])
+            assert pin_dst[o:o + int(l1[i])].tobytes() == wb
+            assert page_dst[o:o + int(l2[i])].tobytes() == wb
