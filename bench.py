@@ -338,7 +338,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config1", choices=["config1", "config0", "config2", "config3", "config4"])
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
-    ap.add_argument("--workers", type=int, default=16, help="config4: server workers (streams)")
+    ap.add_argument("--workers", type=int, default=8, help="config4: server workers (streams)")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--blocks", type=int, default=0,

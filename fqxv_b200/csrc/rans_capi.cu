@@ -210,6 +210,9 @@ uint64_t enc_bound_one(uint64_t n, int order) {
     return kHdr + tables + kStatesBytes + 2 * n;
 }
 
+// Smallest batch output written in place into a pinned host destination.
+constexpr uint64_t kZeroCopyMinBytes = 4ull << 20;
+
 // Device address of a pinned, mapped host buffer (nullptr for any other
 // memory): with unified addressing a kernel can load and store it directly.
 void *mapped_device_ptr(const void *h) {
@@ -762,16 +765,15 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
         end = std::max<uint64_t>(end, blocks[i].offset + blocks[i].length);
         oend = std::max<uint64_t>(oend, out_spans[i].offset + out_spans[i].length);
     }
-    // Pinned (mapped) host buffers are read and written by the kernels in
-    // place over the host link, so the transfers overlap the decode instead
-    // of preceding and following it; other buffers are staged by copies.
-    const uint8_t *d_in = static_cast<const uint8_t *>(mapped_device_ptr(h_src));
-    uint8_t *d_out = static_cast<uint8_t *>(mapped_device_ptr(h_dst));
-    if (!d_in) {
-        CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
-        CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
-        d_in = ctx->io_in.as<uint8_t>();
-    }
+    // The compressed input is staged by one copy (the decoders' word reads
+    // are latency-sensitive); a pinned (mapped) destination of a large batch
+    // is written by the kernels in place over the host link, so the output
+    // transfer overlaps the decode instead of following it (stores are
+    // posted, nothing waits on them). Other destinations are staged.
+    CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
+    CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
+    const uint8_t *d_in = ctx->io_in.as<uint8_t>();
+    uint8_t *d_out = oend >= kZeroCopyMinBytes ? static_cast<uint8_t *>(mapped_device_ptr(h_dst)) : nullptr;
     const bool staged_out = d_out == nullptr;
     if (staged_out) {
         CK(ctx->io_out.ensure(std::max<uint64_t>(oend, 16), s));

@@ -112,7 +112,10 @@ namespace {
 // context's device arenas are in place.
 void warm_worker(fqxv_rans_ctx *ctx, HostPinned &h_in, HostPinned &h_out) {
     const size_t n = 1 << 16;
-    if (!h_in.ensure(32u << 20) || !h_out.ensure(32u << 20)) return;
+    // 64 MiB each way covers a request of the largest usual size without
+    // pinning more memory on the request path (pinning costs about half a
+    // millisecond per MiB); larger batches grow the buffers geometrically.
+    if (!h_in.ensure(64u << 20) || !h_out.ensure(64u << 20)) return;
     uint8_t *src = static_cast<uint8_t *>(h_in.p);
     uint32_t z = 12345;
     for (size_t i = 0; i < n; i++) {

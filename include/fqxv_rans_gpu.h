@@ -166,12 +166,12 @@ int fqxv_rans_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_
 
 /* Host-buffer batch forms of the two calls above: the input arena is copied
  * to the device, coded in one pass, and the results copied back (pinned host
- * memory makes the copies asynchronous DMA). For decode, pinned (mapped)
- * source and destination buffers are instead read and written by the
- * kernels in place over the host link, overlapping the transfers with the
- * decode; the destination bytes of a stream that fails are then
- * unspecified. out_spans/out_lens/status as above; for encode, out_spans
- * index into h_dst. */
+ * memory makes the copies asynchronous DMA). For decode, a pinned (mapped)
+ * destination of at least 4 MiB is instead written by the kernels in place
+ * over the host link, overlapping the output transfer with the decode; the
+ * destination bytes of a stream that fails are then unspecified.
+ * out_spans/out_lens/status as above; for encode, out_spans index into
+ * h_dst. */
 int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
                                 size_t nblocks, int order, uint8_t *h_dst, uint64_t dst_cap,
                                 fqxv_rans_span *out_spans, int32_t *out_orders);

@@ -143,8 +143,8 @@ def test_decode_batch_per_block_status(codec, orc):
 
 
 def test_host_decode_pinned_and_pageable_agree(codec, orc):
-    """Pinned buffers are decoded in place by the kernels, pageable ones
-    through staging copies; both give the oracle's bytes and statuses."""
+    """A pinned destination is written in place by the kernels, a pageable
+    one through a staging copy; both give the oracle's bytes and statuses."""
     import torch
 
     rng = np.random.default_rng(9)
