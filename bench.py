@@ -16,6 +16,8 @@ Workloads (seeded synthetic data of the benchmark shapes):
   config0  1 x 1 MiB binned quality, order-0
   config2  4096 mixed blocks 4 KiB - 4 MiB, both orders, keep the smaller
   config3  config2 (CPU-encoded) + ONT long-read blocks, decode only
+  batch0 / batch1 / batch1f   2048 x 512 KiB binned order-0 / binned order-1 /
+           full-range order-1: peak batched throughput of one order
 
 The reference arm (`--impl reference`) times the reference's CPU coder -- the
 C restatement of fqxv-rans (AVX-512/AVX2 order-0, scalar order-1) -- with all
@@ -55,6 +57,13 @@ def build_workload(name: str, seed: int, blocks: int = 0):
     if name == "config0":
         data, spans = W.config0(seed=seed)
         return data, spans, 0, "1 x 1 MiB binned quality block, order-0", {}
+    if name in ("batch0", "batch1", "batch1f"):
+        # peak batched throughput of one order: 2048 x 512 KiB (1 GiB)
+        kind = "full" if name == "batch1f" else "binned"
+        order = 0 if name == "batch0" else 1
+        nb = blocks or 2048
+        data, spans = W.uniform_batch(kind, nblocks=nb, seed=seed)
+        return data, spans, order, "%d x 512 KiB %s quality, order-%d" % (nb, "full-range" if kind == "full" else "binned", order), {}
     workers = min(32, os.cpu_count() or 1)
     if name == "config2":
         nb = blocks or 4096
@@ -386,7 +395,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config1", choices=["config1", "config0", "config2", "config3", "config4"])
+    ap.add_argument("--workload", default="config1",
+                    choices=["config1", "config0", "config2", "config3", "config4", "batch0", "batch1", "batch1f"])
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
     ap.add_argument("--workers", type=int, default=8, help="config4: server workers (streams)")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])

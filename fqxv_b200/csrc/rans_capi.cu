@@ -773,7 +773,27 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
     CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
     CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
     const uint8_t *d_in = ctx->io_in.as<uint8_t>();
-    uint8_t *d_out = oend >= kZeroCopyMinBytes ? static_cast<uint8_t *>(mapped_device_ptr(h_dst)) : nullptr;
+    // In place only while the decode's output rate stays under what the host
+    // link takes as small stores (about 30 GB/s was still faster in place
+    // than a copy afterwards, measured on B200); faster batches are
+    // better served by one bulk copy afterwards. The decode time is
+    // estimated from the stream headers: the largest stream's serial rounds
+    // (about 320 ns per 32 bytes for order-1, 80 ns for order-0 on B200) or
+    // the whole batch at the batched rates (about 15 and 300 GB/s).
+    double t_lat = 0.0, b0 = 0.0, b1 = 0.0;
+    for (size_t i = 0; i < nblocks; i++) {
+        if (blocks[i].length < kHdr) continue;
+        const uint8_t *h = h_src + blocks[i].offset;
+        uint64_t n = 0;
+        for (int k = 0; k < 8; k++) n |= (uint64_t)h[1 + k] << (8 * k);
+        if (n > out_spans[i].length) continue;
+        const bool o1 = h[0] == 1;
+        t_lat = std::max(t_lat, (double)(n / 32) * (o1 ? 320e-9 : 80e-9));
+        (o1 ? b1 : b0) += (double)n;
+    }
+    const double t_est = std::max(t_lat, b1 / 15e9 + b0 / 300e9);
+    const bool in_place = oend >= kZeroCopyMinBytes && t_est > 0.0 && (double)oend / t_est < 40e9;
+    uint8_t *d_out = in_place ? static_cast<uint8_t *>(mapped_device_ptr(h_dst)) : nullptr;
     const bool staged_out = d_out == nullptr;
     if (staged_out) {
         CK(ctx->io_out.ensure(std::max<uint64_t>(oend, 16), s));

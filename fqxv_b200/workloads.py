@@ -158,6 +158,14 @@ def _gen_one(args):
     return GENERATORS[name](size, seed)
 
 
+def uniform_batch(kind: str, nblocks: int = 2048, block: int = 512 * KiB, seed: int = 0):
+    """Many equal blocks of one stream type (binned or full-range quality):
+    the shape for peak batched throughput of one order and direction."""
+    gen = binned_quality if kind == "binned" else full_quality
+    data = gen(nblocks * block, seed)
+    return data, _spans([block] * nblocks)
+
+
 def config2(nblocks: int = 4096, lo: int = 4 * KiB, hi: int = 4 * MiB, seed: int = 0, workers: int = 0):
     """Mixed blocks, sizes log-uniform in [lo, hi], stream type uniform over
     the four generators; block i is seeded with seed + i. `workers` > 1

@@ -168,8 +168,10 @@ int fqxv_rans_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_
  * to the device, coded in one pass, and the results copied back (pinned host
  * memory makes the copies asynchronous DMA). For decode, a pinned (mapped)
  * destination of at least 4 MiB is instead written by the kernels in place
- * over the host link, overlapping the output transfer with the decode; the
- * destination bytes of a stream that fails are then unspecified.
+ * over the host link when the batch decodes slowly enough for the link
+ * (estimated from the stream headers), overlapping the output transfer with
+ * the decode; the destination bytes of a stream that fails are then
+ * unspecified.
  * out_spans/out_lens/status as above; for encode, out_spans index into
  * h_dst. */
 int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
