@@ -78,10 +78,11 @@ constexpr int kGroups = 6;  // decode launch groups
 
 enum Stage {
     kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
-    kStages
+    kStDecO1Small, kStages
 };
 const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan", "enc_pack",
-                                          "dec_parse", "dec_o0", "dec_o1_dense", "dec_o1_global"};
+                                          "dec_parse", "dec_o0", "dec_o1_dense", "dec_o1_global",
+                                          "dec_o1_small"};
 
 // CUDA-event brackets around each kernel launch on the context's stream.
 // Durations are collected after the call's final synchronisation.
@@ -417,13 +418,14 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     {
         // Launch groups: order-0; order-1 dense by alphabet size (the shared
         // memory of a group is its largest member's, so small alphabets get
-        // many CTAs per SM); order-1 global.
+        // many CTAs per SM; the smallest decode with one warp per stream);
+        // order-1 global.
         const DecStream *ps = reinterpret_cast<const DecStream *>(hst);
         auto group_of = [&](const DecStream &d) -> int {
             if (d.cls == kClsO0) return 0;
             if (d.cls == kClsO1Global) return kGroups - 1;
             if (d.cls != kClsO1Dense) return -1;
-            return d.nd <= 7 ? 1 : d.nd <= 15 ? 2 : d.nd <= 31 ? 3 : 4;
+            return d.nd <= kSmallMaxNd ? 1 : d.nd <= 15 ? 2 : d.nd <= 31 ? 3 : 4;
         };
         std::vector<uint32_t> lists[kGroups];
         uint32_t smem[kGroups] = {};
@@ -432,7 +434,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             const int g = group_of(ps[i]);
             if (g < 0) continue;
             lists[g].push_back(i);
-            smem[g] = std::max(smem[g], dec_smem_bytes(ps[i].cls, ps[i].nd));
+            smem[g] = std::max(smem[g], dec_smem_bytes(g == 1 ? kClsO1Small : ps[i].cls, ps[i].nd));
             cbytes[g] += ps[i].src_len + ps[i].n;
         }
         size_t tot = 0;
@@ -452,8 +454,9 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         for (int g = 0; g < kGroups; g++) {
             const size_t m = lists[g].size();
             if (!m) continue;
-            const int cls = g == 0 ? kClsO0 : g == kGroups - 1 ? kClsO1Global : kClsO1Dense;
-            const int stage = g == 0 ? kStDecO0 : g == kGroups - 1 ? kStDecO1Global : kStDecO1Dense;
+            const int cls = g == 0 ? kClsO0 : g == kGroups - 1 ? kClsO1Global : g == 1 ? kClsO1Small : kClsO1Dense;
+            const int stage = g == 0 ? kStDecO0 : g == kGroups - 1 ? kStDecO1Global : g == 1 ? kStDecO1Small
+                                                                                              : kStDecO1Dense;
             cudaStream_t as = ctx->aux[g];
             CK(cudaStreamWaitEvent(as, ctx->ev_fork, 0));
             int per_sm = dec_blocks_per_sm(cls, smem[g]);

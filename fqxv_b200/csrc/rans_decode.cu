@@ -604,6 +604,18 @@ __global__ void __launch_bounds__(32)
 // parameter) plus, on lane 0 of every warp, segment 0; the rows go to a
 // double-buffered shared array, and after the barrier every warp resolves
 // the round itself. Only warp 0 stores the output.
+constexpr int kO1Warps = 4;
+constexpr int kO1Threads = 32 * kO1Warps;
+constexpr int kO1Workers = kO1Threads - kO1Warps;  // threads that run speculative chains
+
+__device__ __forceinline__ void named_bar(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kO1Threads) : "memory");
+}
+
+// The rounds of one order-1 dense stream (scalar.rs:202-215), shared by the
+// 4-warp and the 1-warp decoders: `resolve(slot, d, ctx)` runs one round's
+// context chain and gives this lane's symbol and context; `store` says
+// whether this warp writes the output.
 //
 // Rounds that cannot run out of words (and are not the first or the partial
 // last round) take a branch-free fast path: the ring advances by predication,
@@ -611,12 +623,88 @@ __global__ void __launch_bounds__(32)
 // run of fast rounds -- such a stream fails anyway, and a truncation cannot
 // come earlier inside those rounds. Other rounds take the careful path with
 // every check of scalar.rs:202-215 in order.
-constexpr int kO1Warps = 4;
-constexpr int kO1Threads = 32 * kO1Warps;
-constexpr int kO1Workers = kO1Threads - kO1Warps;  // threads that run speculative chains
-
-__device__ __forceinline__ void named_bar(int id) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kO1Threads) : "memory");
+template <class Resolve>
+__device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__restrict__ out, uint32_t lt,
+                                         const uint32_t *__restrict__ FC, const uint8_t *__restrict__ DS,
+                                         uint32_t stride, uint32_t dead, bool store, uint32_t x,
+                                         Resolve &&resolve) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t n = S.n;
+    const uint64_t navail = S.words_len / 2;
+    uint64_t wp = 0;
+    const uint64_t rounds = (n + 31) / 32, full = n / 32;
+    uint64_t r = 0;
+    int status = FQXV_RANS_OK;
+    while (r < rounds && status == FQXV_RANS_OK) {
+        const int64_t spare = (int64_t)navail - (int64_t)wp - 64;
+        int64_t cnt = spare > 0 ? spare / 32 : 0;
+        const int64_t left_full = r < full ? (int64_t)(full - r) : 0;
+        if (cnt > left_full) cnt = left_full;
+        if (r == 0 || cnt <= 0) {
+            // careful round (scalar.rs:202-215 in order)
+            R.advance(wp);
+            const uint64_t i = r * 32 + lane;
+            const bool active = i < n;
+            const uint32_t slot = x & (kTotFreq - 1);
+            uint32_t d, ctx;
+            resolve(slot, d, ctx);
+            const uint32_t deadmask = __ballot_sync(0xffffffffu, active && d == dead);
+            const int absent_at = deadmask ? __ffs(deadmask) - 1 : 32;
+            const bool valid = active && lane < absent_at;
+            const uint32_t fc = FC[ctx * stride + d];
+            uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
+            const bool need = valid && v < kRansL;
+            if (!renorm_round(v, need, R, wp, navail, lt, r == 0)) {
+                status = FQXV_RANS_E_TRUNCATED;
+                break;
+            }
+            if (absent_at < 32) {
+                status = FQXV_RANS_E_ABSENT_CONTEXT;
+                break;
+            }
+            if (active) {
+                if (store) out[i] = DS[d];
+                x = v;
+            }
+            r++;
+            continue;
+        }
+        // fast rounds: each takes at most 32 words, cnt of them fit.
+        R.advance(wp);
+        uint32_t w32 = (uint32_t)wp;
+        uint32_t adv_at = (uint32_t)((512u * (uint32_t)(R.next_seg - 3) - R.lead + 1u) / 2u);
+        uint32_t sawdead = 0;
+        uint8_t *op = out + r * 32 + lane;
+        for (int64_t c = 0; c < cnt; c++) {
+            // predicated one-segment ring advance (a round moves <= 64 bytes)
+            const bool adv = w32 - (uint32_t)wp >= adv_at - (uint32_t)wp;
+            if (adv) {
+                R.put(R.next_seg, R.pend);
+                R.next_seg++;
+                R.pend = R.fetch(R.next_seg);
+                adv_at += 256u;
+            }
+            __syncwarp();
+            const uint32_t cand = R.word(w32 + lane);
+            const uint32_t slot = x & (kTotFreq - 1);
+            uint32_t d, ctx;
+            resolve(slot, d, ctx);
+            sawdead |= d == dead;
+            const uint32_t fc = FC[ctx * stride + d];
+            const uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
+            const bool need = v < kRansL;
+            const uint32_t mask = __ballot_sync(0xffffffffu, need);
+            const uint32_t w = __shfl_sync(0xffffffffu, cand, __popc(mask & lt) & 31);
+            if (store) *op = DS[d];
+            op += 32;
+            x = need ? (v << 16) | w : v;
+            w32 += __popc(mask);
+        }
+        wp += (uint32_t)(w32 - (uint32_t)wp);
+        r += (uint64_t)cnt;
+        if (__any_sync(0xffffffffu, sawdead != 0)) status = FQXV_RANS_E_ABSENT_CONTEXT;
+    }
+    return status;
 }
 
 // Rows of the speculative chains, 16 bytes each: the eight chain values
@@ -659,12 +747,8 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         rows[0][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
         rows[1][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
     }
-    const uint64_t n = S.n;
-    const uint64_t navail = S.words_len / 2;
-    uint32_t x = S.states[lane];
-    uint64_t wp = 0;
+    const uint32_t x = S.states[lane];
     uint32_t din = (uint32_t)S.start;
-    const uint64_t rounds = (n + 31) / 32, full = n / 32;
     const int seg = lane >> 3, pos = lane & 7;
     const uint32_t shd = 24u - 8u * (uint32_t)(pos & 3);        // byte pos of a row half
     const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);  // byte pos - 1
@@ -718,78 +802,7 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         buf ^= 1u;
     };
 
-    uint64_t r = 0;
-    int status = FQXV_RANS_OK;
-    while (r < rounds && status == FQXV_RANS_OK) {
-        const int64_t spare = (int64_t)navail - (int64_t)wp - 64;
-        int64_t cnt = spare > 0 ? spare / 32 : 0;
-        const int64_t left_full = r < full ? (int64_t)(full - r) : 0;
-        if (cnt > left_full) cnt = left_full;
-        if (r == 0 || cnt <= 0) {
-            // careful round (scalar.rs:202-215 in order)
-            R.advance(wp);
-            const uint64_t i = r * 32 + lane;
-            const bool active = i < n;
-            const uint32_t slot = x & (kTotFreq - 1);
-            uint32_t d, ctx;
-            resolve(slot, d, ctx);
-            const uint32_t deadmask = __ballot_sync(0xffffffffu, active && d == dead);
-            const int absent_at = deadmask ? __ffs(deadmask) - 1 : 32;
-            const bool valid = active && lane < absent_at;
-            const uint32_t fc = FC[ctx * stride + d];
-            uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
-            const bool need = valid && v < kRansL;
-            if (!renorm_round(v, need, R, wp, navail, lt, r == 0)) {
-                status = FQXV_RANS_E_TRUNCATED;
-                break;
-            }
-            if (absent_at < 32) {
-                status = FQXV_RANS_E_ABSENT_CONTEXT;
-                break;
-            }
-            if (active) {
-                if (warp == 0) out[i] = DS[d];
-                x = v;
-            }
-            r++;
-            continue;
-        }
-        // fast rounds: each takes at most 32 words, cnt of them fit.
-        R.advance(wp);
-        uint32_t w32 = (uint32_t)wp;
-        uint32_t adv_at = (uint32_t)((512u * (uint32_t)(R.next_seg - 3) - R.lead + 1u) / 2u);
-        uint32_t sawdead = 0;
-        uint8_t *op = out + r * 32 + lane;
-        for (int64_t c = 0; c < cnt; c++) {
-            // predicated one-segment ring advance (a round moves <= 64 bytes)
-            const bool adv = w32 - (uint32_t)wp >= adv_at - (uint32_t)wp;
-            if (adv) {
-                R.put(R.next_seg, R.pend);
-                R.next_seg++;
-                R.pend = R.fetch(R.next_seg);
-                adv_at += 256u;
-            }
-            __syncwarp();
-            const uint32_t cand = R.word(w32 + lane);
-            const uint32_t slot = x & (kTotFreq - 1);
-            uint32_t d, ctx;
-            resolve(slot, d, ctx);
-            sawdead |= d == dead;
-            const uint32_t fc = FC[ctx * stride + d];
-            const uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
-            const bool need = v < kRansL;
-            const uint32_t mask = __ballot_sync(0xffffffffu, need);
-            const uint32_t w = __shfl_sync(0xffffffffu, cand, __popc(mask & lt) & 31);
-            if (warp == 0) *op = DS[d];
-            op += 32;
-            x = need ? (v << 16) | w : v;
-            w32 += __popc(mask);
-        }
-        wp += (uint32_t)(w32 - (uint32_t)wp);
-        r += (uint64_t)cnt;
-        if (__any_sync(0xffffffffu, sawdead != 0)) status = FQXV_RANS_E_ABSENT_CONTEXT;
-    }
-    return status;
+    return o1_rounds(S, R, out, lt, FC, DS, stride, dead, warp == 0, x, resolve);
 }
 
 __global__ void __launch_bounds__(kO1Threads, 1)
@@ -832,6 +845,106 @@ __global__ void __launch_bounds__(kO1Threads, 1)
                                     : o1d_stream<2>(S, sm, R, s_rows, out, lt);
         if (tid == 0) S.status = status;
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// order-1, small alphabets (|D| <= kSmallMaxNd): one warp per stream
+// ---------------------------------------------------------------------------
+
+// The same four segments of eight, but every chain fits in one warp: lane 0
+// runs segment 0 from the known context, lanes 1..3 nd run segment s >= 1
+// from every possible incoming context (lane 1 + (s - 1) nd + c), lane 31
+// holds the DEAD row. Each row carries the lane of the row the next segment
+// continues from, so resolving a round is three dependent shuffles -- no
+// shared rows, no barrier, no copies of the states. With tables of a few
+// tens of KB, several streams share an SM.
+__device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
+                                          uint8_t *__restrict__ out, uint32_t lt) {
+    const int lane = threadIdx.x & 31;
+    const int nd = S.nd;
+    const uint32_t dead = (uint32_t)nd;
+    const bool task = lane >= 1 && lane <= 3 * nd;
+    const uint32_t myseg = task ? (uint32_t)(1 + (lane - 1) / nd) : 0u;
+    const uint32_t myc = task ? (uint32_t)((lane - 1) % nd) : 0u;
+    const uint32_t nbase = 1u + myseg * (uint32_t)nd;  // lane of the next segment's context-0 row
+    const uint8_t *CT = sm;
+    const uint32_t stride = (uint32_t)nd + 1;
+    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
+    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
+    const uint32_t deadw = 0x01010101u * dead;
+    uint32_t din = (uint32_t)S.start;
+    const int seg = lane >> 3, pos = lane & 7;
+    const uint32_t shd = 24u - 8u * (uint32_t)(pos & 3);
+    const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);
+
+    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
+        uint32_t sl[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, slot, 8 * myseg + k);
+        uint32_t dd = lane == 0 ? din : myc;
+        uint32_t hi = 0, lo = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            dd = CT[dd * kChainStride + sl[k]];
+            hi = hi * 256u + dd;
+        }
+#pragma unroll
+        for (int k = 4; k < 8; k++) {
+            dd = CT[dd * kChainStride + sl[k]];
+            lo = lo * 256u + dd;
+        }
+        uint32_t nx = dd == dead ? 31u : nbase + dd;
+        if (lane == 31) {
+            hi = deadw;
+            lo = deadw;
+            nx = 31u;
+        }
+        const uint32_t r0x = __shfl_sync(0xffffffffu, hi, 0), r0y = __shfl_sync(0xffffffffu, lo, 0);
+        const uint32_t n0 = __shfl_sync(0xffffffffu, nx, 0);
+        const uint32_t r1x = __shfl_sync(0xffffffffu, hi, n0), r1y = __shfl_sync(0xffffffffu, lo, n0);
+        const uint32_t n1 = __shfl_sync(0xffffffffu, nx, n0);
+        const uint32_t r2x = __shfl_sync(0xffffffffu, hi, n1), r2y = __shfl_sync(0xffffffffu, lo, n1);
+        const uint32_t n2 = __shfl_sync(0xffffffffu, nx, n1);
+        const uint32_t rx = seg == 0 ? r0x : seg == 1 ? r1x : r2x;
+        const uint32_t ry = seg == 0 ? r0y : seg == 1 ? r1y : r2y;
+        const uint32_t ine = seg == 0 ? din : seg == 1 ? (r0y & 0xffu) : (r1y & 0xffu);
+        const uint32_t r3x = __shfl_sync(0xffffffffu, hi, n2), r3y = __shfl_sync(0xffffffffu, lo, n2);
+        const uint32_t row_x = seg == 3 ? r3x : rx;
+        const uint32_t row_y = seg == 3 ? r3y : ry;
+        const uint32_t in = seg == 3 ? (r2y & 0xffu) : ine;
+        d = ((pos < 4 ? row_x : row_y) >> shd) & 0xffu;
+        ctx = pos == 0 ? in : ((pos <= 4 ? row_x : row_y) >> shc) & 0xffu;
+        din = r3y & 0xffu;
+    };
+    return o1_rounds(S, R, out, lt, FC, DS, stride, dead, true, S.states[lane], resolve);
+}
+
+__global__ void __launch_bounds__(32)
+    dec_o1s_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
+                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
+                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
+    extern __shared__ __align__(128) uint8_t sm[];
+    __shared__ __align__(8) uint64_t bar;
+    const int lane = threadIdx.x;
+    const uint32_t lt = lanemask_lt();
+    TableStager st;
+    st.init(&bar);
+    for (;;) {
+        const int j = pop_job(queue);
+        if (j >= nlist) return;
+        DecStream &S = streams[list[j]];
+        st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
+        WordRing R;
+        R.init(src + S.words_off, S.words_len, sm + ring_off);
+        if (!st.wait()) {
+            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
+            st.wait();
+            return;
+        }
+        const int status = o1s_stream(S, sm, R, dst + S.dst_off, lt);
+        if (lane == 0) S.status = status;
+        __syncwarp();
     }
 }
 
@@ -924,6 +1037,7 @@ uint32_t dec_smem_bytes(int cls, int nd) {
         case kClsO0: return 16384 + kRingBytes;
         case kClsO1Dense: return (uint32_t)align_up(dense_table_bytes(nd), 128) + kO1Warps * kRingBytes;
         case kClsO1Global: return kRingBytes;
+        case kClsO1Small: return (uint32_t)align_up(dense_table_bytes(nd), 128) + kRingBytes;
         default: return 0;
     }
 }
@@ -948,6 +1062,8 @@ static void ensure_dec_attrs() {
                          (int)dec_smem_bytes(kClsO1Dense, kDenseMax));
     cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)dec_smem_bytes(kClsO1Global, 0));
+    cudaFuncSetAttribute(dec_o1s_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dec_smem_bytes(kClsO1Small, kSmallMaxNd));
     g_attr_done[dev] = true;
 }
 
@@ -964,6 +1080,9 @@ int dec_blocks_per_sm(int cls, uint32_t smem_bytes) {
             break;
         case kClsO1Global:
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1g_kernel, 32, smem_bytes);
+            break;
+        case kClsO1Small:
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1s_kernel, 32, smem_bytes);
             break;
         default:
             break;
@@ -996,6 +1115,10 @@ void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint3
             break;
         case kClsO1Global:
             dec_o1g_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
+            break;
+        case kClsO1Small:
+            dec_o1s_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
+                                                      smem_bytes - kRingBytes);
             break;
         default:
             break;

@@ -86,6 +86,10 @@ struct DecStream {
 };
 
 enum { kClsNone = 0, kClsO0 = 1, kClsO1Dense = 2, kClsO1Global = 3 };
+// Launch class of dense streams with |D| <= kSmallMaxNd (their tables are the
+// dense layout; one warp decodes a stream).
+constexpr int kClsO1Small = 4;
+constexpr int kSmallMaxNd = 10;
 
 // Decode table arena per stream (bytes from tbl_off).
 //   order-0: 4096 x u32 packed ((freq - 1) << 20) | ((slot - cum) << 8) | sym.
