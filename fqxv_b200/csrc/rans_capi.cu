@@ -156,7 +156,7 @@ struct fqxv_rans_ctx {
     cudaEvent_t ev_fork = nullptr, ev_join[kGroups] = {};
     std::mutex mu;
     // encode
-    DevBuf e_blocks, e_order, e_jobs, e_tbl, e_words, e_hist, e_misc;
+    DevBuf e_blocks, e_order, e_jobs, e_tbl, e_words, e_hist, e_misc, e_keys;
     // decode
     DevBuf d_streams, d_order, d_tbl, d_misc;
     // single-call staging
@@ -165,7 +165,7 @@ struct fqxv_rans_ctx {
     HostBuf h_io;
     StageTimer timer;
     uint64_t device_bytes() const {
-        const DevBuf *all[] = {&e_blocks, &e_order, &e_jobs, &e_tbl, &e_words, &e_hist, &e_misc,
+        const DevBuf *all[] = {&e_blocks, &e_order, &e_jobs, &e_tbl, &e_words, &e_hist, &e_misc, &e_keys,
                                &d_streams, &d_order, &d_tbl, &d_misc, &io_in, &io_out};
         uint64_t t = 0;
         for (auto *b : all) t += b->cap;
@@ -270,6 +270,12 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     CK(ctx->e_tbl.ensure(std::max<uint64_t>(toff, 256), s));
     CK(ctx->e_words.ensure(std::max<uint64_t>(woff * 2, 16), s));
     CK(ctx->e_hist.ensure(o1 ? (size_t)model_grid * 65536 * 4 : 256, s));
+    // order-1: each input position's table index (u16), written by the
+    // model and read by the encode
+    uint64_t src_end = 0;
+    for (size_t i = 0; i < nb; i++) src_end = std::max<uint64_t>(src_end, blocks[i].offset + blocks[i].length);
+    if (o1) CK(ctx->e_keys.ensure(2 * (src_end + 16), s));
+    uint16_t *dK = o1 ? ctx->e_keys.as<uint16_t>() : nullptr;
     CK(ctx->e_misc.ensure((2 + nb) * 16, s));
     // Stage descriptors through pinned memory, one copy per array.
     const size_t szb = nb * sizeof(EncBlock), szo = nb * 4, szj = jobs.size() * sizeof(EncJob);
@@ -295,10 +301,10 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     const int run_grid = ctx->sms * 16;
     if (persistent) {
         cudaEvent_t t0 = ctx->timer.begin(s);
-        CK(launch_enc_model(d_src, dB, dO, (int)nb, dT, dH, model_grid, s));
+        CK(launch_enc_model(d_src, dB, dO, (int)nb, dT, dH, dK, model_grid, s));
         ctx->timer.end(kStEncModel, t0, s);
         t0 = ctx->timer.begin(s);
-        launch_enc_run(d_src, dB, dJ, (int)jobs.size(), dT, dW, queue,
+        launch_enc_run(d_src, dB, dJ, (int)jobs.size(), dT, dW, queue, dK,
                        std::min<int>(run_grid, (int)(jobs.size() + 3) / 4), s);
         ctx->timer.end(kStEncRun, t0, s);
     } else {
@@ -307,10 +313,10 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         for (size_t j = 0; j < nb; j++) {
             CK(cudaMemsetAsync(queue, 0, 4, s));
             cudaEvent_t t0 = ctx->timer.begin(s);
-            CK(launch_enc_model(d_src, dB, dO + j, 1, dT, dH, 1, s));
+            CK(launch_enc_model(d_src, dB, dO + j, 1, dT, dH, dK, 1, s));
             ctx->timer.end(kStEncModel, t0, s);
             t0 = ctx->timer.begin(s);
-            launch_enc_run(d_src, dB, dJ + j * per, per, dT, dW, queue, 1, s);
+            launch_enc_run(d_src, dB, dJ + j * per, per, dT, dW, queue, dK, 1, s);
             ctx->timer.end(kStEncRun, t0, s);
         }
     }
@@ -578,7 +584,7 @@ void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     DevBuf *all[] = {&ctx->e_blocks, &ctx->e_order, &ctx->e_jobs, &ctx->e_tbl, &ctx->e_words,
-                     &ctx->e_hist, &ctx->e_misc, &ctx->d_streams, &ctx->d_order, &ctx->d_tbl,
+                     &ctx->e_hist, &ctx->e_misc, &ctx->e_keys, &ctx->d_streams, &ctx->d_order, &ctx->d_tbl,
                      &ctx->d_misc, &ctx->io_in, &ctx->io_out};
     for (auto *b : all) b->release();
     ctx->h_stage.release();

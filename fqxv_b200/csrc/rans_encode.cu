@@ -34,9 +34,9 @@ __device__ __forceinline__ void unpack16(const uint4 v, uint32_t b[16]) {
 // (one per thread per step) and in single bytes for the unaligned head and
 // the tail. For every byte the visitor gets (previous byte or 0 at position
 // 0, byte); runs of equal keys are folded into one shared-memory atomic.
-template <class KeyFn, class AddFn>
+template <class KeyFn, class AddFn, class EmitFn, class Emit16Fn>
 __device__ __forceinline__ void histogram_pass(const uint8_t *__restrict__ p, uint64_t lo, uint64_t hi, KeyFn key,
-                                               AddFn add) {
+                                               AddFn add, EmitFn emit, Emit16Fn emit16) {
     if (hi <= lo) return;
     const uint64_t n = hi - lo;
     const uint64_t mis = (uint64_t)(uintptr_t)(p + lo) & 15u;
@@ -44,19 +44,30 @@ __device__ __forceinline__ void histogram_pass(const uint8_t *__restrict__ p, ui
     if (head > n) head = n;
     const uint64_t body = (n - head) / 16;
     const uint64_t tail0 = lo + head + body * 16;
-    for (uint64_t i = lo + threadIdx.x; i < lo + head; i += blockDim.x) add(key(i ? p[i - 1] : 0u, p[i]), 1u);
-    for (uint64_t i = tail0 + threadIdx.x; i < hi; i += blockDim.x) add(key(i ? p[i - 1] : 0u, p[i]), 1u);
+    for (uint64_t i = lo + threadIdx.x; i < lo + head; i += blockDim.x) {
+        const uint32_t k = key(i ? p[i - 1] : 0u, p[i]);
+        emit(i, k);
+        add(k, 1u);
+    }
+    for (uint64_t i = tail0 + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint32_t k = key(i ? p[i - 1] : 0u, p[i]);
+        emit(i, k);
+        add(k, 1u);
+    }
     for (uint64_t c = threadIdx.x; c < body; c += blockDim.x) {
         const uint64_t pos = lo + head + 16 * c;
         const uint4 v = __ldg(reinterpret_cast<const uint4 *>(p + pos));
         uint32_t b[16];
         unpack16(v, b);
         uint32_t prev = pos ? (uint32_t)p[pos - 1] : 0u;
+        uint32_t ks[16];
         uint32_t k0 = key(prev, b[0]);
+        ks[0] = k0;
         uint32_t run = 1;
 #pragma unroll
         for (int k = 1; k < 16; k++) {
             const uint32_t kk = key(b[k - 1], b[k]);
+            ks[k] = kk;
             if (kk != k0) {
                 add(k0, run);
                 k0 = kk;
@@ -66,6 +77,7 @@ __device__ __forceinline__ void histogram_pass(const uint8_t *__restrict__ p, ui
             }
         }
         add(k0, run);
+        emit16(pos, ks);
     }
 }
 
@@ -86,7 +98,7 @@ __device__ __forceinline__ uint2 enc_entry(uint32_t f, uint32_t cum) {
 __global__ void __launch_bounds__(kModelThreads)
     enc_model_kernel(const uint8_t *__restrict__ src, EncBlock *__restrict__ blocks,
                      const uint32_t *__restrict__ order, int nblocks, uint8_t *__restrict__ tbl,
-                     uint32_t *__restrict__ hist_scratch) {
+                     uint32_t *__restrict__ hist_scratch, uint16_t *__restrict__ keys) {
     namespace cg = cooperative_groups;
     constexpr int W = kModelThreads / 32;
     constexpr int kSmemU = 64;
@@ -117,7 +129,8 @@ __global__ void __launch_bounds__(kModelThreads)
         uint32_t *hw = h0[warp];
         histogram_pass(
             p, lo, hi, [](uint32_t, uint32_t c) { return c; },
-            [&](uint32_t k, uint32_t r) { atomicAdd(&hw[k], r); });
+            [&](uint32_t k, uint32_t r) { atomicAdd(&hw[k], r); }, [](uint64_t, uint32_t) {},
+            [](uint64_t, const uint32_t *) {});
         __syncthreads();
         if (tid < 256) {
             uint32_t t = 0;
@@ -168,6 +181,19 @@ __global__ void __launch_bounds__(kModelThreads)
         __syncthreads();
         const int nu = s_nu;
         auto pair = [&](uint32_t prev, uint32_t c) { return (uint32_t)umap[prev] * nu + umap[c]; };
+        // the order-1 table index of every position, for the encode (when
+        // the caller gave scratch for it); indexed from src rounded down to
+        // 16 bytes, so a 16-byte input chunk's indices are one aligned 32 B
+        uint16_t *kb = keys ? keys + ((uintptr_t)src & 15u) + blocks[b].src_off : nullptr;
+        auto emit = [&](uint64_t i, uint32_t k) {
+            if (kb) kb[i] = (uint16_t)k;
+        };
+        auto emit16 = [&](uint64_t pos, const uint32_t *k) {
+            if (!kb) return;
+            uint4 *d = reinterpret_cast<uint4 *>(kb + pos);
+            d[0] = make_uint4(k[0] | k[1] << 16, k[2] | k[3] << 16, k[4] | k[5] << 16, k[6] | k[7] << 16);
+            d[1] = make_uint4(k[8] | k[9] << 16, k[10] | k[11] << 16, k[12] | k[13] << 16, k[14] | k[15] << 16);
+        };
         uint2 *T1 = reinterpret_cast<uint2 *>(T + kTblO1);
         if (rank == 0 && tid < 256) T[kTblUmap + tid] = umap[tid];
         if (nu <= kSmemU) {
@@ -175,7 +201,7 @@ __global__ void __launch_bounds__(kModelThreads)
             // the cluster; context rows are spread over all warps of it
             for (int i = tid; i < nu * nu; i += blockDim.x) h1[i] = 0;
             __syncthreads();
-            histogram_pass(p, lo, hi, pair, [&](uint32_t k, uint32_t r) { atomicAdd(&h1[k], r); });
+            histogram_pass(p, lo, hi, pair, [&](uint32_t k, uint32_t r) { atomicAdd(&h1[k], r); }, emit, emit16);
             cl.sync();
             for (int t = warp + W * rank; t < nu; t += W * C) {
                 for (int u = lane; u < nu; u += 32) {
@@ -200,7 +226,7 @@ __global__ void __launch_bounds__(kModelThreads)
             // in global scratch
             for (int i = tid; i < nu * nu; i += blockDim.x) gh[i] = 0;
             __syncthreads();
-            histogram_pass(p, 0, n, pair, [&](uint32_t k, uint32_t r) { atomicAdd(&gh[k], r); });
+            histogram_pass(p, 0, n, pair, [&](uint32_t k, uint32_t r) { atomicAdd(&gh[k], r); }, emit, emit16);
             __syncthreads();
             for (int t = warp; t < nu; t += W) {
                 uint32_t f[8], cum[8];
@@ -266,10 +292,11 @@ __device__ __forceinline__ void enc_emit(bool need, uint32_t word, uint16_t *__r
 // warp vote per round) is kept off the state chain: a chunk records its
 // emit flags and pre-step states, and its words are written while the next
 // chunk's states are computed.
-template <int ORDER, bool SMEM_TAB>
+template <int ORDER, bool SMEM_TAB, bool KEYS>
 __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint64_t n,
                                             const uint2 *__restrict__ tab,
                                             const uint8_t *__restrict__ umap, uint32_t nu,
+                                            const uint16_t *__restrict__ keys,
                                             uint16_t *__restrict__ words, uint64_t word_end,
                                             uint64_t &nwords, uint32_t &state) {
     const int lane = threadIdx.x & 31;
@@ -279,17 +306,21 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
     const int64_t full = (int64_t)(n / 32);
     const uint32_t rem = (uint32_t)(n % 32);
     // Table entry of symbol s with predecessor `prev` (order-1: scalar.rs:85).
+    // With KEYS, `s` is already the position's order-1 table index.
     auto entry = [&](uint32_t s, uint32_t prev) -> uint2 {
         if (ORDER == 0) return tab[s];
-        const uint32_t idx = (uint32_t)umap[prev] * nu + umap[s];
+        const uint32_t idx = KEYS ? s : (uint32_t)umap[prev] * nu + umap[s];
         return SMEM_TAB ? tab[idx] : __ldg(tab + idx);
     };
+    // symbol (or table index) of position i, and its context byte
+    auto sym_at = [&](uint64_t i) -> uint32_t { return KEYS ? (uint32_t)keys[i] : (uint32_t)__ldg(p + i); };
+    constexpr bool CTX = ORDER == 1 && !KEYS;
     if (rem) {
         const uint64_t i = (uint64_t)full * 32 + lane;
         const bool active = lane < (int)rem;
-        const uint32_t s = active ? (uint32_t)__ldg(p + i) : 0u;
+        const uint32_t s = active ? sym_at(i) : 0u;
         uint32_t prev = 0;
-        if (ORDER == 1) prev = (active && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
+        if (CTX) prev = (active && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
         const uint2 e = active ? entry(s, prev) : make_uint2(0u, 0u);
         const uint32_t x_before = x;
         const bool need = enc_step(x, e, active);
@@ -304,25 +335,25 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
     for (int k = 0; k < 16; k++) {
         const int64_t r = full - 1 - k;
         const uint64_t i = (uint64_t)r * 32 + lane;
-        cur[k] = r >= 0 ? (uint32_t)__ldg(p + i) : 0u;
-        curp[k] = (ORDER == 1 && r >= 0 && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
+        cur[k] = r >= 0 ? sym_at(i) : 0u;
+        curp[k] = (CTX && r >= 0 && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
         pwv[k] = 0;
     }
     for (int64_t rt = full - 1; rt >= 0; rt -= 16) {
         if (rt >= 32) {
-            const uint8_t *pc = p + (uint64_t)(rt - 16) * 32 + lane;
+            const uint64_t ic = (uint64_t)(rt - 16) * 32 + lane;
 #pragma unroll
             for (int k = 0; k < 16; k++) {
-                nxt[k] = (uint32_t)__ldg(pc - 32 * k);
-                if (ORDER == 1) nxtp[k] = (uint32_t)__ldg(pc - 32 * k - 1);
+                nxt[k] = sym_at(ic - 32 * k);
+                if (CTX) nxtp[k] = (uint32_t)__ldg(p + ic - 32 * k - 1);
             }
         } else {
 #pragma unroll
             for (int k = 0; k < 16; k++) {
                 const int64_t r = rt - 16 - k;
                 const uint64_t i = (uint64_t)r * 32 + lane;
-                nxt[k] = r >= 0 ? (uint32_t)__ldg(p + i) : 0u;
-                nxtp[k] = (ORDER == 1 && r >= 0 && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
+                nxt[k] = r >= 0 ? sym_at(i) : 0u;
+                nxtp[k] = (CTX && r >= 0 && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
             }
         }
         const bool whole = rt >= 15;
@@ -331,7 +362,7 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
         // chain one round at a time (a warp issues in order).
         uint2 ent[16];
 #pragma unroll
-        for (int k = 0; k < 16; k++) ent[k] = entry(cur[k], ORDER == 1 ? curp[k] : 0u);
+        for (int k = 0; k < 16; k++) ent[k] = entry(cur[k], CTX ? curp[k] : 0u);
         uint32_t bits = 0;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
@@ -362,7 +393,7 @@ constexpr uint32_t kEncO1TabBytes = (kEncO1SmemNu * kEncO1SmemNu * 8 + 127) / 12
 __global__ void __launch_bounds__(kEncWarpsPerCta * 32)
     enc_run_kernel(const uint8_t *__restrict__ src, EncBlock *__restrict__ blocks,
                    const EncJob *__restrict__ jobs, int njobs, const uint8_t *__restrict__ tbl,
-                   uint16_t *__restrict__ words, int *__restrict__ queue) {
+                   uint16_t *__restrict__ words, int *__restrict__ queue, const uint16_t *__restrict__ keys) {
     extern __shared__ __align__(16) uint8_t dsm[];
     __shared__ uint2 s_tab[kEncWarpsPerCta][256];
     __shared__ uint8_t s_umap[kEncWarpsPerCta][256];
@@ -386,7 +417,7 @@ __global__ void __launch_bounds__(kEncWarpsPerCta * 32)
 #pragma unroll
                 for (int k = 0; k < 8; k++) s_tab[warp][lane * 8 + k] = T0[lane * 8 + k];
                 __syncwarp();
-                encode_warp<0, true>(p, n, s_tab[warp], nullptr, 0, words, word_end, nw, st);
+                encode_warp<0, true, false>(p, n, s_tab[warp], nullptr, 0, nullptr, words, word_end, nw, st);
             } else {
 #pragma unroll
                 for (int k = 0; k < 8; k++) s_umap[warp][lane * 8 + k] = T[kTblUmap + lane * 8 + k];
@@ -396,10 +427,18 @@ __global__ void __launch_bounds__(kEncWarpsPerCta * 32)
                     uint2 *t = reinterpret_cast<uint2 *>(dsm + warp * kEncO1TabBytes);
                     for (uint32_t i = lane; i < nu * nu; i += 32) t[i] = T1[i];
                     __syncwarp();
-                    encode_warp<1, true>(p, n, t, s_umap[warp], nu, words, word_end, nw, st);
+                    if (keys)
+                        encode_warp<1, true, true>(p, n, t, s_umap[warp], nu, keys + ((uintptr_t)src & 15u) + B.src_off, words,
+                                                   word_end, nw, st);
+                    else
+                        encode_warp<1, true, false>(p, n, t, s_umap[warp], nu, nullptr, words, word_end, nw, st);
                 } else {
                     __syncwarp();
-                    encode_warp<1, false>(p, n, T1, s_umap[warp], nu, words, word_end, nw, st);
+                    if (keys)
+                        encode_warp<1, false, true>(p, n, T1, s_umap[warp], nu, keys + ((uintptr_t)src & 15u) + B.src_off, words,
+                                                    word_end, nw, st);
+                    else
+                        encode_warp<1, false, false>(p, n, T1, s_umap[warp], nu, nullptr, words, word_end, nw, st);
                 }
             }
         }
@@ -577,7 +616,7 @@ __global__ void __launch_bounds__(kPackThreads)
 }
 
 cudaError_t launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
-                             uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s) {
+                             uint8_t *tbl, uint32_t *hist_scratch, uint16_t *keys, int grid, cudaStream_t s) {
     if (nblocks <= 0) return cudaSuccess;
     // `grid` clusters of kModelCluster CTAs
     cudaLaunchConfig_t cfg = {};
@@ -592,11 +631,12 @@ cudaError_t launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, enc_model_kernel, src, blocks, order, nblocks, tbl, hist_scratch);
+    return cudaLaunchKernelEx(&cfg, enc_model_kernel, src, blocks, order, nblocks, tbl, hist_scratch, keys);
 }
 
 void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,
-                    const uint8_t *tbl, uint16_t *words, int *queue, int grid, cudaStream_t s) {
+                    const uint8_t *tbl, uint16_t *words, int *queue, const uint16_t *keys, int grid,
+                    cudaStream_t s) {
     if (njobs <= 0) return;
     static std::mutex mu;
     static bool done[256];
@@ -613,7 +653,7 @@ void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, in
         }
     }
     enc_run_kernel<<<grid, kEncWarpsPerCta * 32, kEncWarpsPerCta * kEncO1TabBytes, s>>>(src, blocks, jobs, njobs,
-                                                                                       tbl, words, queue);
+                                                                                       tbl, words, queue, keys);
 }
 
 void launch_enc_select_scan(EncBlock *blocks, int nblocks, uint64_t *total, cudaStream_t s) {

@@ -141,11 +141,14 @@ constexpr uint32_t kOutRows = 3 * kDenseMax + 1;
 inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 // ---- launchers (rans_encode.cu / rans_decode.cu) ---------------------------
-// `grid` clusters of kModelCluster CTAs; returns the launch status.
+// `grid` clusters of kModelCluster CTAs; returns the launch status. `keys`
+// (nullable, u16 per input byte) receives each position's order-1 table
+// index for the encode.
 cudaError_t launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
-                             uint8_t *tbl, uint32_t *hist_scratch, int grid, cudaStream_t s);
+                             uint8_t *tbl, uint32_t *hist_scratch, uint16_t *keys, int grid, cudaStream_t s);
 void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,
-                    const uint8_t *tbl, uint16_t *words, int *queue, int grid, cudaStream_t s);
+                    const uint8_t *tbl, uint16_t *words, int *queue, const uint16_t *keys, int grid,
+                    cudaStream_t s);
 void launch_enc_select_scan(EncBlock *blocks, int nblocks, uint64_t *total, cudaStream_t s);
 void launch_enc_pack(EncBlock *blocks, int nblocks, const uint8_t *tbl, const uint16_t *words,
                      uint8_t *dst, int grid, cudaStream_t s);

@@ -127,11 +127,11 @@ extern "C" int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int orde
     const int njobs = (order == FQXV_RANS_BEST_TIE0 || order == FQXV_RANS_BEST_TIE1) ? 2 : 1;
 
     noalloc_setup_kernel<<<1, 32, 0, cs>>>(n, order);
-    if (launch_enc_model(d_src, B, ord, 1, tbl, hist, 1, cs) != cudaSuccess) {
+    if (launch_enc_model(d_src, B, ord, 1, tbl, hist, nullptr, 1, cs) != cudaSuccess) {
         cudaGetLastError();
         return FQXV_RANS_E_CUDA;
     }
-    launch_enc_run(d_src, B, jobs, njobs, tbl, words, queue, 1, cs);
+    launch_enc_run(d_src, B, jobs, njobs, tbl, words, queue, nullptr, 1, cs);
     launch_enc_select_scan(B, 1, total, cs);
     launch_enc_pack(B, 1, tbl, words, d_dst, 1, cs);
     uint64_t len = 0;

@@ -78,7 +78,7 @@ uint64_t request_mem(const Request &r) {
     // Inputs, outputs and the per-block scratch of the batched passes.
     if (r.kind == 0) {
         const uint64_t n = r.in.size();
-        return n + fqxv_rans_encode_bound(n, r.order) + 4 * n + fqxv::enc_table_bytes(n) + (1 << 16);
+        return n + fqxv_rans_encode_bound(n, r.order) + 6 * n + fqxv::enc_table_bytes(n) + (1 << 16);
     }
     return r.in.size() + r.n_out + fqxv::dec_table_bytes(r.in.size()) + (1 << 16);
 }
