@@ -18,6 +18,8 @@ Workloads (seeded synthetic data of the benchmark shapes):
   config3  config2 (CPU-encoded) + ONT long-read blocks, decode only
   batch0 / batch1 / batch1f   2048 x 512 KiB binned order-0 / binned order-1 /
            full-range order-1: peak batched throughput of one order
+  cpu_single (with --impl reference)  the CPU coder on one thread, 8 MiB of
+           quality_like data, per path (the reference's own benchmark shape)
 
 The reference arm (`--impl reference`) times the reference's CPU coder -- the
 C restatement of fqxv-rans (AVX-512/AVX2 order-0, scalar order-1) -- with all
@@ -223,8 +225,47 @@ def cpu_encoded(data, spans, seed_tag):
     return arena, np.stack([offs, elen.astype(np.uint64)], 1)
 
 
+def run_cpu_single(args) -> None:
+    """One thread, 8 MiB of `quality_like` data (the shape of the
+    reference's own criterion benchmarks, benches/rans.rs:11-25): MiB/s of
+    the CPU restatement per path, to set beside the reference's published
+    single-thread figures (lib.rs:15-16, 106-108, 176-178)."""
+    from oracle import oracle
+
+    data = W.quality_like(8 << 20).tobytes()
+    n = len(data)
+    paths = ["scalar"] + (["avx2"] if oracle.simd_level() >= 1 else []) + (["avx512"] if oracle.simd_level() >= 2 else [])
+    rows = {}
+
+    def rate(fn):
+        fn()
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < 1.0 or reps < 3:
+            fn()
+            reps += 1
+        return round(n * reps / (time.perf_counter() - t0) / (1 << 20), 1)
+
+    for path in paths:
+        enc = oracle.encode(data, 0, path=path)
+        rows["order0_encode_" + path] = rate(lambda: oracle.encode(data, 0, path=path))
+        rows["order0_decode_" + path] = rate(lambda: oracle.decode(enc, path=path))
+    enc1 = oracle.encode(data, 1)
+    rows["order1_encode_scalar"] = rate(lambda: oracle.encode(data, 1))
+    rows["order1_decode_scalar"] = rate(lambda: oracle.decode(enc1))
+    line = {"impl": "reference", "metric": "single-thread CPU MiB/s (8 MiB quality_like)", "unit": "MiB/s",
+            "config": {"workload": "cpu_single", "bytes": n, "threads": 1}, "rates": rows,
+            "published_cascade_lake": {"order0_decode_scalar": 163, "order0_decode_avx2": 315,
+                                       "order0_decode_avx512": 817, "order0_encode_scalar": 163,
+                                       "order0_encode_avx512": 233}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
+        return
+    if args.workload == "cpu_single":
+        run_cpu_single(args)
         return
     data, spans, order, desc, extra = build_workload(args.workload, args.seed, args.blocks)
     nthreads = os.cpu_count() or 1
@@ -396,7 +437,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config1",
-                    choices=["config1", "config0", "config2", "config3", "config4", "batch0", "batch1", "batch1f"])
+                    choices=["config1", "config0", "config2", "config3", "config4", "batch0", "batch1", "batch1f",
+                             "cpu_single"])
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
     ap.add_argument("--workers", type=int, default=8, help="config4: server workers (streams)")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
