@@ -173,3 +173,34 @@ def test_host_decode_pinned_and_pageable_agree(codec, orc):
             o = int(doffs[i])
             assert pin_dst[o:o + int(l1[i])].tobytes() == wb
             assert page_dst[o:o + int(l2[i])].tobytes() == wb
+
+
+def test_small_alphabet_order1_statuses_match_oracle(codec, orc):
+    """Order-1 streams of small alphabets (the one-warp decoder): good,
+    truncated and corrupted streams give the oracle's bytes and statuses."""
+    rng = np.random.default_rng(21)
+    streams, want = [], []
+    for i in range(60):
+        k = int(rng.integers(1, 9))
+        blk = rng.integers(0, k, int(rng.integers(1, 40_000))).astype(np.uint8)
+        blk = (blk + 60).tobytes()
+        e = bytearray(orc.encode(blk, 1))
+        if i % 4 == 1:
+            e = e[:int(rng.integers(9, len(e)))]
+        elif i % 4 == 2 and len(e) > 200:
+            for _ in range(3):
+                e[int(rng.integers(41, len(e)))] = int(rng.integers(0, 256))
+        streams.append(bytes(e))
+        want.append(orc.decode_status(bytes(e), max_len=1 << 16))
+    lens = np.array([len(s) for s in streams], np.uint64)
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint64)
+    arena = np.frombuffer(b"".join(streams), np.uint8)
+    caps = np.full(len(streams), 1 << 16, np.uint64)
+    doffs = np.arange(len(streams), dtype=np.uint64) << np.uint64(16)
+    d_dec, olens, st = codec.decode_batch(_dev(arena), np.stack([offs, lens], 1), np.stack([doffs, caps], 1),
+                                          max_len=1 << 16, raise_on_error=False)
+    dec = d_dec.cpu().numpy()
+    for i, (ws, wb) in enumerate(want):
+        assert st[i] == ws, (i, st[i], ws)
+        if ws == 0:
+            assert dec[int(doffs[i]):int(doffs[i]) + int(olens[i])].tobytes() == wb, i
