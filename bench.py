@@ -444,7 +444,7 @@ def main() -> None:
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--blocks", type=int, default=0,
-                    help="configs 1/2: number of blocks (0 = the benchmark shape; smaller for profiler captures)")
+                    help="configs 1/2 and batch*: number of blocks (0 = the benchmark shape; smaller for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
