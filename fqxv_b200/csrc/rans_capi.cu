@@ -7,6 +7,8 @@
 #include <numeric>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "rans_internal.cuh"
 
 using namespace fqxv;
@@ -226,12 +228,20 @@ void *mapped_device_ptr(const void *h) {
     return a.devicePointer;
 }
 
+// NVTX range for the lifetime of a scope: the batch calls and their stages
+// show up by name in a timeline profiler (no cost without one attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
 int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks,
                       size_t nb, int mode, uint8_t *d_dst, uint64_t dst_cap, fqxv_rans_span *out_spans,
                       int32_t *out_orders, int persistent) {
     if (mode < FQXV_RANS_ORDER0 || mode > FQXV_RANS_BEST_TIE1) return FQXV_RANS_E_INVALID_ARG;
     if (nb == 0) return FQXV_RANS_OK;
     if (nb > (1u << 30)) return FQXV_RANS_E_TOO_LARGE;
+    NvtxRange range("fqxv.encode_batch");
     cudaStream_t s = ctx->stream;
     const bool o0 = mode != FQXV_RANS_ORDER1, o1 = mode != FQXV_RANS_ORDER0;
 
@@ -371,6 +381,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
                       int32_t *status, int persistent) {
     if (nb == 0) return FQXV_RANS_OK;
     if (nb > (1u << 30)) return FQXV_RANS_E_TOO_LARGE;
+    NvtxRange range("fqxv.decode_batch");
     cudaStream_t s = ctx->stream;
     std::vector<DecStream> hs(nb);
     uint64_t toff = 0;
@@ -742,6 +753,7 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
                                 fqxv_rans_span *out_spans, int32_t *out_orders) {
     if (!ctx || (nblocks && (!blocks || !out_spans || !h_dst || !h_src))) return FQXV_RANS_E_INVALID_ARG;
     if (nblocks == 0) return FQXV_RANS_OK;
+    NvtxRange range("fqxv.encode_batch_host");
     std::lock_guard<std::mutex> g(ctx->mu);
     DeviceGuard dg(ctx->device);
     cudaStream_t s = ctx->stream;
@@ -766,6 +778,7 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
                                 const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status) {
     if (!ctx || (nblocks && (!blocks || !out_spans || !h_src || !h_dst))) return FQXV_RANS_E_INVALID_ARG;
     if (nblocks == 0) return FQXV_RANS_OK;
+    NvtxRange range("fqxv.decode_batch_host");
     std::lock_guard<std::mutex> g(ctx->mu);
     DeviceGuard dg(ctx->device);
     cudaStream_t s = ctx->stream;
