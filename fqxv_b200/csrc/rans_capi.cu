@@ -1,10 +1,12 @@
 // C ABI of libfqxv_rans_gpu.so: contexts, device arenas, the batched device
 // API and the reference-shaped single-call host API (include/fqxv_rans_gpu.h).
 #include <algorithm>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -166,11 +168,14 @@ struct fqxv_rans_ctx {
     HostBuf h_stage;
     HostBuf h_io;
     StageTimer timer;
+    // host-buffer batches cut into chunks run one chunk per sub-context
+    std::vector<fqxv_rans_ctx *> sub;
     uint64_t device_bytes() const {
         const DevBuf *all[] = {&e_blocks, &e_order, &e_jobs, &e_tbl, &e_words, &e_hist, &e_misc, &e_keys,
                                &d_streams, &d_order, &d_tbl, &d_misc, &io_in, &io_out};
         uint64_t t = 0;
         for (auto *b : all) t += b->cap;
+        for (auto *c : sub) t += c->device_bytes();
         return t;
     }
 };
@@ -592,6 +597,8 @@ int fqxv_rans_ctx_create(int device, fqxv_rans_ctx **out) {
 
 void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
     if (!ctx) return;
+    for (auto *c : ctx->sub) fqxv_rans_ctx_destroy(c);
+    ctx->sub.clear();
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     DevBuf *all[] = {&ctx->e_blocks, &ctx->e_order, &ctx->e_jobs, &ctx->e_tbl, &ctx->e_words,
@@ -748,13 +755,17 @@ int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int
     return FQXV_RANS_OK;
 }
 
-int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
-                                size_t nblocks, int order, uint8_t *h_dst, uint64_t dst_cap,
-                                fqxv_rans_span *out_spans, int32_t *out_orders) {
-    if (!ctx || (nblocks && (!blocks || !out_spans || !h_dst || !h_src))) return FQXV_RANS_E_INVALID_ARG;
-    if (nblocks == 0) return FQXV_RANS_OK;
-    NvtxRange range("fqxv.encode_batch_host");
-    std::lock_guard<std::mutex> g(ctx->mu);
+}  // extern "C"
+
+namespace {
+
+// Encode on one context: input copied in, coded, and -- once `place` gives
+// where this batch's streams go in h_dst (it may wait for an earlier chunk)
+// -- copied out. Offsets of out_spans are local to the batch on entry to
+// `place` and final on return.
+template <class Place>
+int encode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks, size_t nblocks,
+                    int order, fqxv_rans_span *out_spans, int32_t *out_orders, Place &&place) {
     DeviceGuard dg(ctx->device);
     cudaStream_t s = ctx->stream;
     uint64_t end = 0;
@@ -765,21 +776,146 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
     CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
     int st = encode_batch_impl(ctx, ctx->io_in.as<uint8_t>(), blocks, nblocks, order, ctx->io_out.as<uint8_t>(),
                                bound, out_spans, out_orders, 1);
+    const uint64_t total = st ? 0 : out_spans[nblocks - 1].offset + out_spans[nblocks - 1].length;
+    uint8_t *dst = nullptr;
+    const int pst = place(st, total, dst);  // publishes this batch's end for the next chunk
     if (st) return st;
-    const uint64_t total = out_spans[nblocks - 1].offset + out_spans[nblocks - 1].length;
-    if (total > dst_cap) return FQXV_RANS_E_DST_TOO_SMALL;
-    CK(cudaMemcpyAsync(h_dst, ctx->io_out.p, total, cudaMemcpyDeviceToHost, s));
+    if (pst) return pst;
+    CK(cudaMemcpyAsync(dst, ctx->io_out.p, total, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return FQXV_RANS_OK;
 }
 
-int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
-                                size_t nblocks, uint64_t max_len, uint8_t *h_dst,
-                                const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status) {
-    if (!ctx || (nblocks && (!blocks || !out_spans || !h_src || !h_dst))) return FQXV_RANS_E_INVALID_ARG;
+// Host-buffer batches of at least kPipeMinBytes are cut into up to
+// kPipeChunks chunks of consecutive blocks, each coded by its own
+// sub-context on its own host thread: one chunk's copies overlap the other
+// chunks' kernels, and chunks of equal blocks run side by side on the GPU.
+constexpr uint64_t kPipeMinBytes = 32ull << 20;
+constexpr int kPipeChunks = 4;
+
+// [first, last) block ranges of roughly equal bytes
+std::vector<std::pair<size_t, size_t>> pipe_chunks(const fqxv_rans_span *blocks, size_t n) {
+    std::vector<std::pair<size_t, size_t>> out;
+    uint64_t total = 0;
+    for (size_t i = 0; i < n; i++) total += blocks[i].length;
+    if (total < kPipeMinBytes || n < 2) {
+        out.emplace_back(0, n);
+        return out;
+    }
+    const int k = (int)std::min<size_t>(kPipeChunks, n);
+    size_t b = 0;
+    uint64_t acc = 0;
+    for (int c = 0; c < k && b < n; c++) {
+        const uint64_t target = total * (uint64_t)(c + 1) / (uint64_t)k;
+        size_t e = b + 1;
+        acc += blocks[b].length;
+        while (e < n && (c == k - 1 || acc + blocks[e].length <= target)) acc += blocks[e++].length;
+        out.emplace_back(b, e);
+        b = e;
+    }
+    if (b < n) out.back().second = n;
+    return out;
+}
+
+// The sub-contexts of a context (created on first use, same device).
+int ensure_subs(fqxv_rans_ctx *ctx, size_t k) {
+    while (ctx->sub.size() < k) {
+        fqxv_rans_ctx *c = nullptr;
+        const int st = fqxv_rans_ctx_create(ctx->device, &c);
+        if (st != FQXV_RANS_OK) return st;
+        ctx->sub.push_back(c);
+    }
+    return FQXV_RANS_OK;
+}
+
+// Rebased copy of spans [b, e): offsets relative to the first byte any of
+// them touches; returns that byte's offset.
+uint64_t rebase(const fqxv_rans_span *spans, size_t b, size_t e, std::vector<fqxv_rans_span> &out) {
+    uint64_t lo = UINT64_MAX;
+    for (size_t i = b; i < e; i++) lo = std::min<uint64_t>(lo, spans[i].offset);
+    if (lo == UINT64_MAX) lo = 0;
+    out.resize(e - b);
+    for (size_t i = b; i < e; i++) out[i - b] = {spans[i].offset - lo, spans[i].length};
+    return lo;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
+                                size_t nblocks, int order, uint8_t *h_dst, uint64_t dst_cap,
+                                fqxv_rans_span *out_spans, int32_t *out_orders) {
+    if (!ctx || (nblocks && (!blocks || !out_spans || !h_dst || !h_src))) return FQXV_RANS_E_INVALID_ARG;
+    if (order < FQXV_RANS_ORDER0 || order > FQXV_RANS_BEST_TIE1) return FQXV_RANS_E_INVALID_ARG;
     if (nblocks == 0) return FQXV_RANS_OK;
-    NvtxRange range("fqxv.decode_batch_host");
+    NvtxRange range("fqxv.encode_batch_host");
     std::lock_guard<std::mutex> g(ctx->mu);
+    const auto chunks = pipe_chunks(blocks, nblocks);
+    if (chunks.size() == 1) {
+        return encode_host_one(ctx, h_src, blocks, nblocks, order, out_spans, out_orders,
+                               [&](int st, uint64_t total, uint8_t *&dst) -> int {
+                                   if (st) return st;
+                                   if (total > dst_cap) return FQXV_RANS_E_DST_TOO_SMALL;
+                                   dst = h_dst;
+                                   return FQXV_RANS_OK;
+                               });
+    }
+    const size_t k = chunks.size();
+    int cst = ensure_subs(ctx, k);
+    if (cst != FQXV_RANS_OK) return cst;
+    // chunk c's streams follow chunk c-1's: each chunk publishes where its
+    // output ends as soon as its encode is done, before its own copy out
+    std::mutex pm;
+    std::condition_variable pcv;
+    std::vector<uint64_t> ends(k + 1, 0);
+    std::vector<int> ready(k + 1, 0), sts(k, FQXV_RANS_OK);
+    ready[0] = 1;
+    bool failed = false;
+    std::vector<std::thread> th;
+    for (size_t c = 0; c < k; c++) {
+        th.emplace_back([&, c] {
+            const size_t b = chunks[c].first, e = chunks[c].second;
+            std::vector<fqxv_rans_span> local;
+            const uint64_t lo = rebase(blocks, b, e, local);
+            sts[c] = encode_host_one(ctx->sub[c], h_src + lo, local.data(), e - b, order, out_spans + b,
+                                     out_orders + b, [&](int st, uint64_t total, uint8_t *&dst) -> int {
+                                         std::unique_lock<std::mutex> lk(pm);
+                                         pcv.wait(lk, [&] { return ready[c] != 0; });
+                                         int r = FQXV_RANS_OK;
+                                         if (st || failed) {
+                                             failed = true;
+                                             r = st ? st : FQXV_RANS_E_INVALID_ARG;
+                                         } else if (ends[c] + total > dst_cap) {
+                                             failed = true;
+                                             r = FQXV_RANS_E_DST_TOO_SMALL;
+                                         } else {
+                                             dst = h_dst + ends[c];
+                                             for (size_t i = b; i < e; i++) out_spans[i].offset += ends[c];
+                                             ends[c + 1] = ends[c] + total;
+                                         }
+                                         ready[c + 1] = 1;
+                                         pcv.notify_all();
+                                         return r;
+                                     });
+        });
+    }
+    for (auto &t : th) t.join();
+    // the first failing chunk in block order decides (a later chunk that only
+    // stopped because an earlier one failed reports that one's status)
+    for (size_t c = 0; c < k; c++)
+        if (sts[c] != FQXV_RANS_OK) return sts[c];
+    return FQXV_RANS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Decode on one context (the caller holds its lock).
+int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks, size_t nblocks,
+                    uint64_t max_len, uint8_t *h_dst, const fqxv_rans_span *out_spans, uint64_t *out_lens,
+                    int32_t *status) {
     DeviceGuard dg(ctx->device);
     cudaStream_t s = ctx->stream;
     uint64_t end = 0, oend = 0;
@@ -852,6 +988,46 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
         if (status) status[i] = sts[i];
     }
     return first;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
+                                size_t nblocks, uint64_t max_len, uint8_t *h_dst,
+                                const fqxv_rans_span *out_spans, uint64_t *out_lens, int32_t *status) {
+    if (!ctx || (nblocks && (!blocks || !out_spans || !h_src || !h_dst))) return FQXV_RANS_E_INVALID_ARG;
+    if (nblocks == 0) return FQXV_RANS_OK;
+    NvtxRange range("fqxv.decode_batch_host");
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const auto chunks = pipe_chunks(blocks, nblocks);
+    if (chunks.size() == 1)
+        return decode_host_one(ctx, h_src, blocks, nblocks, max_len, h_dst, out_spans, out_lens, status);
+    const size_t k = chunks.size();
+    const int cst = ensure_subs(ctx, k);
+    if (cst != FQXV_RANS_OK) return cst;
+    std::vector<int> firsts(k, FQXV_RANS_OK);
+    std::vector<std::thread> th;
+    for (size_t c = 0; c < k; c++) {
+        th.emplace_back([&, c] {
+            const size_t b = chunks[c].first, e = chunks[c].second;
+            std::vector<fqxv_rans_span> lin, lout;
+            const uint64_t lo = rebase(blocks, b, e, lin);
+            const uint64_t olo = rebase(out_spans, b, e, lout);
+            firsts[c] = decode_host_one(ctx->sub[c], h_src + lo, lin.data(), e - b, max_len, h_dst + olo,
+                                        lout.data(), out_lens ? out_lens + b : nullptr,
+                                        status ? status + b : nullptr);
+        });
+    }
+    for (auto &t : th) t.join();
+    // a device failure anywhere wins; otherwise the first malformed stream
+    for (size_t c = 0; c < k; c++)
+        if (firsts[c] != FQXV_RANS_OK && (firsts[c] < FQXV_RANS_E_TRUNCATED || firsts[c] > FQXV_RANS_E_TRUNCATED_RENORM))
+            return firsts[c];
+    for (size_t c = 0; c < k; c++)
+        if (firsts[c] != FQXV_RANS_OK) return firsts[c];
+    return FQXV_RANS_OK;
 }
 
 }  // extern "C"

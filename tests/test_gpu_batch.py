@@ -204,3 +204,41 @@ def test_small_alphabet_order1_statuses_match_oracle(codec, orc):
         assert st[i] == ws, (i, st[i], ws)
         if ws == 0:
             assert dec[int(doffs[i]):int(doffs[i]) + int(olens[i])].tobytes() == wb, i
+
+
+def test_host_batches_in_chunks_match_single_pass(codec, orc):
+    """Host-buffer batches of 32 MiB and more run as concurrent chunks; the
+    streams, their placement and per-block statuses equal the one-pass
+    device batch and the oracle, including a malformed stream late in the
+    batch."""
+    import torch
+
+    data, spans = W.config1(nblocks=40, block=1 << 20, seed=4)
+    h_src = torch.from_numpy(data.copy()).pin_memory().numpy()
+    bound = codec.encode_bound(spans, 2)
+    h_enc = torch.zeros(bound, dtype=torch.uint8).pin_memory().numpy()
+    out, orders = codec.encode_batch_host(h_src, spans, 2, h_enc)
+    d_out, sp, _ = codec.encode_batch(_dev(data), spans, 2)
+    assert np.array_equal(out, sp)
+    total = int(sp[-1, 0] + sp[-1, 1])
+    assert np.array_equal(h_enc[:total], d_out[:total].cpu().numpy())
+    for i in (0, 17, 39):
+        o, l = int(sp[i, 0]), int(sp[i, 1])
+        blk = data[int(spans[i, 0]):int(spans[i, 0] + spans[i, 1])].tobytes()
+        e0, e1 = orc.encode(blk, 0), orc.encode(blk, 1)
+        assert h_enc[o:o + l].tobytes() == (e1 if len(e1) < len(e0) else e0)
+    # decode in chunks, with block 37 truncated
+    enc = h_enc[:total].copy()
+    bad = sp.copy()
+    bad[37, 1] = bad[37, 1] // 2
+    h_in = torch.from_numpy(enc).pin_memory().numpy()
+    h_dec = torch.zeros(len(data), dtype=torch.uint8).pin_memory().numpy()
+    lens, st = codec.decode_batch_host(h_in, bad, spans, h_dec, raise_on_error=False)
+    stream37 = enc[int(bad[37, 0]):int(bad[37, 0] + bad[37, 1])].tobytes()
+    assert st[37] == orc.decode_status(stream37)[0] != 0
+    for i in range(40):
+        if i == 37:
+            continue
+        assert st[i] == 0 and lens[i] == spans[i, 1]
+        o, l = int(spans[i, 0]), int(spans[i, 1])
+        assert np.array_equal(h_dec[o:o + l], data[o:o + l]), i
