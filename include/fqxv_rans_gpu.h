@@ -171,7 +171,9 @@ int fqxv_rans_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_
  * over the host link when the batch decodes slowly enough for the link
  * (estimated from the stream headers), overlapping the output transfer with
  * the decode; the destination bytes of a stream that fails are then
- * unspecified.
+ * unspecified. Batches of 32 MiB or more run as up to four concurrent chunks
+ * of consecutive blocks (the context's lock is held throughout), overlapping
+ * one chunk's transfers with another's kernels.
  * out_spans/out_lens/status as above; for encode, out_spans index into
  * h_dst. */
 int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks,
