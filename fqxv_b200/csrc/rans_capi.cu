@@ -452,13 +452,23 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         std::vector<uint32_t> lists[kGroups];
         uint32_t smem[kGroups] = {};
         uint64_t cbytes[kGroups] = {};
+        uint64_t maxn[kGroups] = {};
         for (uint32_t i : ord) {
             const int g = group_of(ps[i]);
             if (g < 0) continue;
             lists[g].push_back(i);
             smem[g] = std::max(smem[g], dec_smem_bytes(g == 1 ? kClsO1Small : ps[i].cls, ps[i].nd));
             cbytes[g] += ps[i].src_len + ps[i].n;
+            maxn[g] = std::max<uint64_t>(maxn[g], ps[i].n);
         }
+        // Groups are launched longest first -- by the serial time of their
+        // largest stream (rounds x cycles per round: ~620 for order-1,
+        // ~160 for order-0) -- so the streams that bound the batch take SMs
+        // before the groups that finish early.
+        int glaunch[kGroups];
+        for (int g = 0; g < kGroups; g++) glaunch[g] = g;
+        auto gcost = [&](int g) { return (double)maxn[g] * (g == 0 ? 160.0 : 620.0); };
+        std::stable_sort(glaunch, glaunch + kGroups, [&](int a, int b) { return gcost(a) > gcost(b); });
         size_t tot = 0;
         for (int g = 0; g < kGroups; g++) tot += lists[g].size();
         CK(ctx->d_order.ensure(std::max<size_t>(tot, 1) * 4, s));
@@ -473,7 +483,8 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         CK(cudaMemsetAsync(queue, 0, 4 * 4 * kGroups, s));
         CK(cudaEventRecord(ctx->ev_fork, s));
         const uint32_t *dl = ctx->d_order.as<uint32_t>();
-        for (int g = 0; g < kGroups; g++) {
+        for (int gi = 0; gi < kGroups; gi++) {
+            const int g = glaunch[gi];
             const size_t m = lists[g].size();
             if (!m) continue;
             const int cls = g == 0 ? kClsO0 : g == kGroups - 1 ? kClsO1Global : g == 1 ? kClsO1Small : kClsO1Dense;
