@@ -277,8 +277,15 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         if (o1) jobs.push_back({b, 1});
         if (o0) jobs.push_back({b, 0});
     }
-    // clusters of the model kernel: as many as are resident at once
-    const int model_grid = (int)std::min<size_t>(nb, std::max<size_t>(1, (size_t)ctx->sms * 4 / kModelCluster));
+    // The model kernel: blocks of kModelClusterMin bytes or more get a
+    // cluster of kModelCluster CTAs each, smaller ones one CTA each (a
+    // cluster's barriers would cost more than their histogram); as many
+    // clusters as are resident at once.
+    size_t nlarge = 0;
+    while (nlarge < nb && hb[ord[nlarge]].n >= kModelClusterMin) nlarge++;
+    const int grid_large = (int)std::min<size_t>(nlarge, std::max<size_t>(1, (size_t)ctx->sms * 4 / kModelCluster));
+    const int grid_small = (int)std::min<size_t>(nb - nlarge, (size_t)ctx->sms * 2);
+    const int model_grid = std::max(grid_large, grid_small);
     CK(ctx->e_blocks.ensure(nb * sizeof(EncBlock), s));
     CK(ctx->e_order.ensure(nb * sizeof(uint32_t), s));
     CK(ctx->e_jobs.ensure(jobs.size() * sizeof(EncJob), s));
@@ -315,9 +322,17 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     uint32_t *dH = ctx->e_hist.as<uint32_t>();
     const int run_grid = ctx->sms * 16;
     if (persistent) {
-        cudaEvent_t t0 = ctx->timer.begin(s);
-        CK(launch_enc_model(d_src, dB, dO, (int)nb, dT, dH, dK, model_grid, s));
-        ctx->timer.end(kStEncModel, t0, s);
+        cudaEvent_t t0;
+        if (nlarge) {
+            t0 = ctx->timer.begin(s);
+            CK(launch_enc_model(d_src, dB, dO, (int)nlarge, dT, dH, dK, grid_large, kModelCluster, s));
+            ctx->timer.end(kStEncModel, t0, s);
+        }
+        if (nb > nlarge) {
+            t0 = ctx->timer.begin(s);
+            CK(launch_enc_model(d_src, dB, dO + nlarge, (int)(nb - nlarge), dT, dH, dK, grid_small, 1, s));
+            ctx->timer.end(kStEncModel, t0, s);
+        }
         t0 = ctx->timer.begin(s);
         launch_enc_run(d_src, dB, dJ, (int)jobs.size(), dT, dW, queue, dK,
                        std::min<int>(run_grid, (int)(jobs.size() + 3) / 4), s);
@@ -328,7 +343,7 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         for (size_t j = 0; j < nb; j++) {
             CK(cudaMemsetAsync(queue, 0, 4, s));
             cudaEvent_t t0 = ctx->timer.begin(s);
-            CK(launch_enc_model(d_src, dB, dO + j, 1, dT, dH, dK, 1, s));
+            CK(launch_enc_model(d_src, dB, dO + j, 1, dT, dH, dK, 1, kModelCluster, s));
             ctx->timer.end(kStEncModel, t0, s);
             t0 = ctx->timer.begin(s);
             launch_enc_run(d_src, dB, dJ + j * per, per, dT, dW, queue, dK, 1, s);

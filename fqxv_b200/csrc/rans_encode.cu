@@ -616,17 +616,18 @@ __global__ void __launch_bounds__(kPackThreads)
 }
 
 cudaError_t launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
-                             uint8_t *tbl, uint32_t *hist_scratch, uint16_t *keys, int grid, cudaStream_t s) {
+                             uint8_t *tbl, uint32_t *hist_scratch, uint16_t *keys, int grid, int cluster,
+                             cudaStream_t s) {
     if (nblocks <= 0) return cudaSuccess;
-    // `grid` clusters of kModelCluster CTAs
+    // `grid` clusters of `cluster` CTAs
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)grid * kModelCluster, 1, 1);
+    cfg.gridDim = dim3((unsigned)grid * (unsigned)cluster, 1, 1);
     cfg.blockDim = dim3(kModelThreads, 1, 1);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kModelCluster;
+    attr[0].val.clusterDim.x = (unsigned)cluster;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;

@@ -24,7 +24,8 @@ constexpr uint64_t kStatesBytes = 4 * kStates;
 
 // Persistent-kernel shapes.
 constexpr int kModelThreads = 512;          // model kernel: threads per CTA
-constexpr int kModelCluster = 8;            // model kernel: CTAs (one cluster) per block
+constexpr int kModelCluster = 8;            // model kernel: CTAs (one cluster) per large block
+constexpr uint64_t kModelClusterMin = 256 << 10;  // smaller blocks get one CTA each
 constexpr int kEncWarpsPerCta = 4;          // encode: one warp per (block, order)
 constexpr int kDecWarpsPerCta = 4;          // decode: one warp per stream
 constexpr int kParseThreads = 256;          // decode header/table kernel
@@ -141,11 +142,12 @@ constexpr uint32_t kOutRows = 3 * kDenseMax + 1;
 inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 // ---- launchers (rans_encode.cu / rans_decode.cu) ---------------------------
-// `grid` clusters of kModelCluster CTAs; returns the launch status. `keys`
-// (nullable, u16 per input byte) receives each position's order-1 table
-// index for the encode.
+// `grid` clusters of `cluster` CTAs (1..8) over the blocks order[0, nblocks);
+// returns the launch status. `keys` (nullable, u16 per input byte) receives
+// each position's order-1 table index for the encode.
 cudaError_t launch_enc_model(const uint8_t *src, EncBlock *blocks, const uint32_t *order, int nblocks,
-                             uint8_t *tbl, uint32_t *hist_scratch, uint16_t *keys, int grid, cudaStream_t s);
+                             uint8_t *tbl, uint32_t *hist_scratch, uint16_t *keys, int grid, int cluster,
+                             cudaStream_t s);
 void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, int njobs,
                     const uint8_t *tbl, uint16_t *words, int *queue, const uint16_t *keys, int grid,
                     cudaStream_t s);

@@ -127,7 +127,7 @@ extern "C" int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int orde
     const int njobs = (order == FQXV_RANS_BEST_TIE0 || order == FQXV_RANS_BEST_TIE1) ? 2 : 1;
 
     noalloc_setup_kernel<<<1, 32, 0, cs>>>(n, order);
-    if (launch_enc_model(d_src, B, ord, 1, tbl, hist, nullptr, 1, cs) != cudaSuccess) {
+    if (launch_enc_model(d_src, B, ord, 1, tbl, hist, nullptr, 1, kModelCluster, cs) != cudaSuccess) {
         cudaGetLastError();
         return FQXV_RANS_E_CUDA;
     }
