@@ -905,7 +905,7 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
             std::vector<fqxv_rans_span> local;
             const uint64_t lo = rebase(blocks, b, e, local);
             sts[c] = encode_host_one(ctx->sub[c], h_src + lo, local.data(), e - b, order, out_spans + b,
-                                     out_orders + b, [&](int st, uint64_t total, uint8_t *&dst) -> int {
+                                     out_orders + b, [&, c](int st, uint64_t total, uint8_t *&dst) -> int {
                                          std::unique_lock<std::mutex> lk(pm);
                                          pcv.wait(lk, [&] { return ready[c] != 0; });
                                          int r = FQXV_RANS_OK;
@@ -924,6 +924,14 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
                                          pcv.notify_all();
                                          return r;
                                      });
+            // a chunk that stopped before placing its output (a failed copy
+            // or allocation) still releases the chunks after it
+            std::lock_guard<std::mutex> lk(pm);
+            if (!ready[c + 1]) {
+                failed = true;
+                ready[c + 1] = 1;
+                pcv.notify_all();
+            }
         });
     }
     for (auto &t : th) t.join();
