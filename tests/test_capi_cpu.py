@@ -76,3 +76,25 @@ def test_status_numbering_matches_oracle():
     opairs = dict(re.findall(r"ORC_(E_\w+) = (\d+)", o))
     for k, v in opairs.items():
         assert pairs[k] == v, k
+
+
+def _build_c_caller(tmp_path):
+    """Compile tests/c/capi_roundtrip.c as strict C99 against the header and
+    link it with the library; returns the executable's path."""
+    import subprocess
+
+    from fqxv_b200 import build
+
+    lib = build.build()
+    libdir = os.path.dirname(lib)
+    exe = str(tmp_path / "capi_roundtrip")
+    cmd = ["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "c", "capi_roundtrip.c"), "-o", exe, "-L", libdir, "-lfqxv_rans_gpu",
+           "-Wl,-rpath," + libdir]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return exe
+
+
+def test_plain_c_caller_compiles_and_links(tmp_path):
+    assert os.path.exists(_build_c_caller(tmp_path))

@@ -176,3 +176,16 @@ def test_multiword_renorm_states(gpu, orc):
             e2[hdr + 4 * lane:hdr + 4 * lane + 4] = (0).to_bytes(4, "little")
             want = orc.decode_status(bytes(e2), max_len=len(data))
             assert _status(gpu.decode_bounded, bytes(e2), len(data)) == want
+
+
+@pytest.mark.gpu
+def test_plain_c_caller_round_trips(tmp_path):
+    """The C ABI from a C99 program (no Python in between): both orders
+    round-trip and the bounded decode rejects an inflated length."""
+    import subprocess
+
+    from test_capi_cpu import _build_c_caller
+
+    r = subprocess.run([_build_c_caller(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "order 1:" in r.stdout
