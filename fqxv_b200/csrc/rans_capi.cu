@@ -218,8 +218,10 @@ uint64_t enc_bound_one(uint64_t n, int order) {
     return kHdr + tables + kStatesBytes + 2 * n;
 }
 
-// Smallest batch output written in place into a pinned host destination.
+// Smallest batch output written in place into a pinned host destination,
+// and fewest streams whose pinned input is read in place.
 constexpr uint64_t kZeroCopyMinBytes = 4ull << 20;
+constexpr size_t kZeroCopyMinStreams = 256;
 
 // Device address of a pinned, mapped host buffer (nullptr for any other
 // memory): with unified addressing a kernel can load and store it directly.
@@ -957,14 +959,12 @@ int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
         end = std::max<uint64_t>(end, blocks[i].offset + blocks[i].length);
         oend = std::max<uint64_t>(oend, out_spans[i].offset + out_spans[i].length);
     }
-    // The compressed input is staged by one copy (the decoders' word reads
+    // The compressed input of a batch of fewer than kZeroCopyMinStreams
+    // streams is staged by one copy, issued first (the decoders' word reads
     // are latency-sensitive); a pinned (mapped) destination of a large batch
     // is written by the kernels in place over the host link, so the output
     // transfer overlaps the decode instead of following it (stores are
     // posted, nothing waits on them). Other destinations are staged.
-    CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
-    CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
-    const uint8_t *d_in = ctx->io_in.as<uint8_t>();
     // In place only while the decode's output rate stays under what the host
     // link takes as small stores (about 30 GB/s was still faster in place
     // than a copy afterwards, measured on B200); faster batches are
@@ -972,6 +972,14 @@ int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
     // estimated from the stream headers: the largest stream's serial rounds
     // (about 320 ns per 32 bytes for order-1, 80 ns for order-0 on B200) or
     // the whole batch at the batched rates (about 15 and 300 GB/s).
+    const uint8_t *d_in = nullptr;
+    auto stage_input = [&]() -> cudaError_t {
+        cudaError_t e = ctx->io_in.ensure(std::max<uint64_t>(end, 16), s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s);
+        d_in = ctx->io_in.as<uint8_t>();
+        return e;
+    };
+    if (nblocks < kZeroCopyMinStreams) CK(stage_input());
     double t_lat = 0.0, b0 = 0.0, b1 = 0.0;
     for (size_t i = 0; i < nblocks; i++) {
         if (blocks[i].length < kHdr) continue;
@@ -986,6 +994,15 @@ int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
     const double t_est = std::max(t_lat, b1 / 15e9 + b0 / 300e9);
     const bool in_place = oend >= kZeroCopyMinBytes && t_est > 0.0 && (double)oend / t_est < 40e9;
     uint8_t *d_out = in_place ? static_cast<uint8_t *>(mapped_device_ptr(h_dst)) : nullptr;
+    // A slow batch of hundreds of streams also reads its pinned input in
+    // place: each stream's words are fetched 16 bytes a lane, segments ahead
+    // of use, at a small share of the link, and the decode starts without
+    // waiting for a copy. Measured on B200: 4103 mixed streams (64 KiB to
+    // 4 MiB) e2e 17.2 -> 21.2 GB/s, but chunks of 16 x 1 MiB order-1 streams
+    // 4.63 -> 4.36, so smaller batches (and single serving requests) keep
+    // the staged copy, issued before the estimate above.
+    if (!d_in && d_out) d_in = static_cast<const uint8_t *>(mapped_device_ptr(h_src));
+    if (!d_in) CK(stage_input());
     const bool staged_out = d_out == nullptr;
     if (staged_out) {
         CK(ctx->io_out.ensure(std::max<uint64_t>(oend, 16), s));
