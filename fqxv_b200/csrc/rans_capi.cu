@@ -997,7 +997,7 @@ int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
     // A slow batch of hundreds of streams also reads its pinned input in
     // place: each stream's words are fetched 16 bytes a lane, segments ahead
     // of use, at a small share of the link, and the decode starts without
-    // waiting for a copy. Measured on B200: 4103 mixed streams (64 KiB to
+    // waiting for a copy. Measured on B200: 4103 mixed streams (4 KiB to
     // 4 MiB) e2e 17.2 -> 21.2 GB/s, but chunks of 16 x 1 MiB order-1 streams
     // 4.63 -> 4.36, so smaller batches (and single serving requests) keep
     // the staged copy, issued before the estimate above.
