@@ -20,6 +20,9 @@ Workloads (seeded synthetic data of the benchmark shapes):
            full-range order-1: peak batched throughput of one order
   cpu_single (with --impl reference)  the CPU coder on one thread, 8 MiB of
            quality_like data, per path (the reference's own benchmark shape)
+  crc      CRC-32C of 4096 payloads 4 KiB - 4 MiB (crates/fqxv/src/crc.rs)
+  frame    block frames of the same payloads: write (copy + CRC-32C, terminator)
+           then read back with every CRC verified (container/block.rs)
 
 The reference arm (`--impl reference`) times the reference's CPU coder -- the
 C restatement of fqxv-rans (AVX-512/AVX2 order-0, scalar order-1) -- with all
@@ -81,6 +84,230 @@ def build_workload(name: str, seed: int, blocks: int = 0):
         return data, spans, None, "config2 blocks (CPU-encoded, best order) + ONT quality blocks (order-1), decode", \
             {"n_ont_blocks": int(len(s3))}
     raise SystemExit("unknown workload %s" % name)
+
+
+FRAME_METRICS = {
+    "crc": "CRC-32C GB/s, bit-exact (payload bytes checksummed per second)",
+    "frame": "block frames write + verified read GB/s, bit-exact (payload bytes per second)",
+}
+
+
+def frame_workload(seed: int, blocks: int = 0):
+    """4096 payloads (log-uniform 4 KiB - 4 MiB, about 2.4 GB) of seeded random
+    bytes: the size range of container block payloads, and random bytes stand
+    for coded streams (the CRC does the same work on any bytes)."""
+    nb = blocks or 4096
+    rng = np.random.default_rng(1000 + seed)
+    sizes = np.exp(rng.uniform(np.log(4 << 10), np.log(4 << 20), nb)).astype(np.uint64)
+    total = int(sizes.sum())
+    data = np.frombuffer(rng.bytes(total), dtype=np.uint8)
+    offs = np.zeros(nb, dtype=np.uint64)
+    offs[1:] = np.cumsum(sizes)[:-1]
+    return data, np.stack([offs, sizes], axis=1), "%d payloads 4 KiB-4 MiB, random bytes" % nb
+
+
+def frame_cpu_step(kind, data, spans, nthreads):
+    """The CPU path over the same payloads: CRC-32C of each (crc); or frames
+    written (CRC + copy) and read back with each CRC verified (frame)."""
+    from oracle import oracle
+
+    if kind == "crc":
+        oracle.crc32c_batch(data, spans[:, 0], spans[:, 1], nthreads)
+        return
+    crcs = oracle.crc32c_batch(data, spans[:, 0], spans[:, 1], nthreads)
+    frames = np.empty(int(spans[:, 1].sum()) + 16 * len(spans) + 12, dtype=np.uint8)
+    fo = np.zeros(len(spans), dtype=np.uint64)
+    fo[1:] = np.cumsum(spans[:, 1] + 16)[:-1]
+    for (o, ln), f in zip(spans, fo):
+        frames[int(f) + 16:int(f) + 16 + int(ln)] = data[int(o):int(o + ln)]
+    got = oracle.crc32c_batch(frames, fo + 16, spans[:, 1], nthreads)
+    assert (got == crcs).all()
+
+
+def run_frames(args, rank: int, world: int, local: int, dist) -> None:
+    import torch
+
+    from fqxv_b200.batch import Codec
+
+    kind = args.workload
+    data, spans, desc = frame_workload(args.seed + rank, args.blocks)
+    n_bytes = int(spans[:, 1].sum())
+    codec = Codec(local)
+    cs = torch.cuda.ExternalStream(codec.stream_handle)
+    d_src = torch.from_numpy(data).to("cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    need = codec.frame_bound(spans, True)
+    d_fr = torch.empty(need, dtype=torch.uint8, device="cuda") if kind == "frame" else None
+
+    def step():
+        if kind == "crc":
+            return codec.crc32c_batch(d_src, spans)
+        _, fo, crcs, total = codec.frame_blocks(d_src, spans, True, d_dst=d_fr)
+        pay, rcrcs, st, consumed, term = codec.read_blocks(d_fr, total)
+        assert term and consumed == total and not st.any() and (rcrcs == crcs).all()
+        return crcs
+
+    from oracle import oracle
+
+    for _ in range(args.warmup):
+        crcs = step()
+    torch.cuda.synchronize()
+    sample = np.linspace(0, len(spans) - 1, 48).astype(int)
+    want = [oracle.crc32c(data[int(spans[i, 0]):int(spans[i, 0] + spans[i, 1])]) for i in sample]
+    assert [int(crcs[i]) for i in sample] == want, "CRC mismatch against the oracle"
+    if kind == "frame":
+        fo = np.zeros(len(spans), dtype=np.uint64)
+        fo[1:] = np.cumsum(spans[:, 1] + 16)[:-1]
+        for i in sample[:8]:
+            a, ln = int(fo[i]) + 16, int(spans[i, 1])
+            assert torch.equal(d_fr[a:a + ln], d_src[int(spans[i, 0]):int(spans[i, 0]) + ln]), "frame copy mismatch"
+
+    codec.stage_stats(reset=True)
+    codec.set_profiling(True)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cs)
+        step()
+        b.record(cs)
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    codec.set_profiling(False)
+    stages = codec.stage_stats(reset=True)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t[0])
+    value = world * n_bytes * args.steps / (total_ms * 1e-3) / 1e9
+
+    pk = peaks()
+    timed = {k: v for k, v in stages.items() if v["launches"] > 0}
+    dom = max(timed, key=lambda k: timed[k]["ms"])
+    launches = timed[dom]["launches"]
+    per_launch_ms = timed[dom]["ms"] / launches
+    # Algorithmic bytes: the CRC pass reads each payload byte once; the frame
+    # copy reads it and writes it once.
+    alg_bytes = timed[dom]["bytes"] / launches
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            ent = json.load(f).get(kind, {}).get(dom)
+        if ent:
+            traffic = ent.get("dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 5), "traffic": traffic,
+                "alg_bytes_per_launch": int(alg_bytes), "launch_ms": round(per_launch_ms, 4),
+                "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"}
+    gpu_launches = int(sum(v["launches"] for v in stages.values()))
+
+    # end to end through the C ABI with pinned host buffers
+    h_src = torch.from_numpy(data).pin_memory().numpy()
+    h_fr = torch.empty(need, dtype=torch.uint8).pin_memory().numpy() if kind == "frame" else None
+
+    def e2e_step():
+        if kind == "crc":
+            return codec.crc32c_batch_host(h_src, spans)
+        fo, crcs, total = codec.frame_blocks_host(h_src, spans, h_fr, True)
+        pay, rcrcs, st, consumed, term = codec.read_blocks_host(h_fr, total)
+        assert term and not st.any() and (rcrcs == crcs).all()
+        return crcs
+
+    c = e2e_step()
+    assert [int(c[i]) for i in sample] == want, "e2e CRC mismatch"
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cs)
+        e2e_step()
+        b.record(cs)
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t[0])
+    e2e = {"value": round(world * n_bytes * args.steps / (e2e_ms * 1e-3) / 1e9, 4), "unit": "GB/s",
+           "h2d_bytes_per_step": n_bytes if kind == "crc" else n_bytes + need,
+           "d2h_bytes_per_step": 4 * len(spans) if kind == "crc" else need + 4 * len(spans),
+           "path": ("fqxv_crc32c_batch_host" if kind == "crc" else
+                    "fqxv_frame_blocks_host + fqxv_read_blocks_host") + " (pinned host buffers)"}
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        nthreads = os.cpu_count() or 1
+        sub = spans[:len(spans) // 4]
+        sub_bytes = int(sub[:, 1].sum())
+        frame_cpu_step(kind, data, sub, nthreads)
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            frame_cpu_step(kind, data, sub, nthreads)
+            reps += 1
+            if time.perf_counter() - t0 > 10.0 or reps >= 10:
+                break
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(sub_bytes * reps / dt / 1e9, 4), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": "%d passes over the first quarter of the payloads (%d bytes): the reference's byte-table "
+                         "CRC-32C (crc.rs:19-79, restated in C)%s on %d host threads over payloads" %
+                         (reps, sub_bytes, "" if kind == "crc" else " + frame copy + verified read", nthreads)}
+
+    if rank == 0:
+        line = {
+            "metric": FRAME_METRICS[kind], "value": round(value, 4), "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": kind, "desc": desc, "blocks": int(len(spans)), "bytes_per_gpu": n_bytes,
+                       "l2": "flushed (256 MiB write) before every timed step",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "bytes": v["bytes"]}
+                       for k, v in stages.items()},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    codec.close()
+
+
+def run_frames_reference(args) -> None:
+    kind = args.workload
+    data, spans, desc = frame_workload(args.seed, args.blocks)
+    nthreads = os.cpu_count() or 1
+    sub = spans[:len(spans) // 4]
+    n_bytes = int(sub[:, 1].sum())
+    for _ in range(args.warmup):
+        frame_cpu_step(kind, data, sub, nthreads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        frame_cpu_step(kind, data, sub, nthreads)
+    dt = time.perf_counter() - t0
+    gbs = n_bytes * args.steps / dt / 1e9
+    line = {
+        "impl": "reference", "metric": FRAME_METRICS[kind], "value": round(gbs, 4), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": kind, "desc": desc, "blocks": int(len(spans)), "bytes": int(spans[:, 1].sum()),
+                   "timed_sample_bytes": n_bytes},
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": nthreads, "kind": "port",
+                         "sample": "the first quarter of the payloads every step: byte-table CRC-32C (crc.rs:19-79, "
+                                   "restated in C) on all host threads over payloads"},
+        "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
 
 
 def peaks() -> dict:
@@ -267,6 +494,9 @@ def run_reference(args, rank: int) -> None:
     if args.workload == "cpu_single":
         run_cpu_single(args)
         return
+    if args.workload in FRAME_METRICS:
+        run_frames_reference(args)
+        return
     data, spans, order, desc, extra = build_workload(args.workload, args.seed, args.blocks)
     nthreads = os.cpu_count() or 1
     n_bytes = int(spans[:, 1].sum())
@@ -438,7 +668,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config1",
                     choices=["config1", "config0", "config2", "config3", "config4", "batch0", "batch1", "batch1f",
-                             "cpu_single"])
+                             "cpu_single", "crc", "frame"])
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
     ap.add_argument("--workers", type=int, default=8, help="config4: server workers (streams)")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
@@ -476,6 +706,13 @@ def main() -> None:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+
+    if args.workload in FRAME_METRICS:
+        run_frames(args, rank, world, local, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     data, spans, order, desc, extra = build_workload(args.workload, args.seed + rank, args.blocks)
     n_bytes = int(spans[:, 1].sum())

@@ -20,6 +20,12 @@ class StageStat(ctypes.Structure):
                 ("bytes", ctypes.c_uint64)]
 
 
+# format.rs:252-266 StreamLoc, as include/fqxv_frame_gpu.h lays it out.
+STREAM_LOC = np.dtype([("offset", "<u8"), ("len", "<u4"), ("crc", "<u4")])
+# Frame statuses (include/fqxv_frame_gpu.h): per-frame results, not call failures.
+FRAME_STATUSES = {32, 33, 34, 35}
+
+
 def _spans(a) -> np.ndarray:
     a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64).reshape(-1, 2))
     return a
@@ -125,6 +131,95 @@ class Codec:
         if st and (raise_on_error or st not in rans.MALFORMED):
             rans.raise_for(st)
         return lens, status
+
+    # ---- CRC-32C and block frames (include/fqxv_frame_gpu.h) --------------
+
+    def crc32c_batch(self, d_src, spans) -> np.ndarray:
+        """CRC-32C (crates/fqxv/src/crc.rs:74) of each span of the device
+        tensor d_src."""
+        s = _spans(spans)
+        out = np.zeros(len(s), dtype=np.uint32)
+        rans.raise_for(self._lib.fqxv_crc32c_batch(self._h, d_src.data_ptr(), s.ctypes.data, len(s),
+                                                   out.ctypes.data))
+        return out
+
+    def crc32c_batch_host(self, h_src: np.ndarray, spans) -> np.ndarray:
+        s = _spans(spans)
+        out = np.zeros(len(s), dtype=np.uint32)
+        rans.raise_for(self._lib.fqxv_crc32c_batch_host(self._h, h_src.ctypes.data, s.ctypes.data, len(s),
+                                                        out.ctypes.data))
+        return out
+
+    def frame_bound(self, spans, terminate: bool = False) -> int:
+        s = _spans(spans)
+        return self._lib.fqxv_frame_blocks_bound(s.ctypes.data, len(s), 1 if terminate else 0)
+
+    def frame_blocks(self, d_src, spans, terminate: bool = False, d_dst=None):
+        """Frame the payloads `spans` of d_src back to back
+        (crates/fqxv/src/container/block.rs:110-142). Returns (d_dst,
+        frame_offsets, crcs, total)."""
+        import torch
+
+        s = _spans(spans)
+        need = self.frame_bound(s, terminate)
+        if d_dst is None:
+            d_dst = torch.empty(max(need, 1), dtype=torch.uint8, device=d_src.device)
+        offs = np.zeros(len(s), dtype=np.uint64)
+        crcs = np.zeros(len(s), dtype=np.uint32)
+        tot = ctypes.c_uint64(0)
+        rans.raise_for(self._lib.fqxv_frame_blocks(self._h, d_src.data_ptr(), s.ctypes.data, len(s),
+                                                   1 if terminate else 0, d_dst.data_ptr(), d_dst.numel(),
+                                                   offs.ctypes.data, crcs.ctypes.data, ctypes.byref(tot)))
+        return d_dst, offs, crcs, tot.value
+
+    def frame_blocks_host(self, h_src: np.ndarray, spans, h_dst: np.ndarray, terminate: bool = False):
+        s = _spans(spans)
+        offs = np.zeros(len(s), dtype=np.uint64)
+        crcs = np.zeros(len(s), dtype=np.uint32)
+        tot = ctypes.c_uint64(0)
+        rans.raise_for(self._lib.fqxv_frame_blocks_host(self._h, h_src.ctypes.data, s.ctypes.data, len(s),
+                                                        1 if terminate else 0, h_dst.ctypes.data, h_dst.size,
+                                                        offs.ctypes.data, crcs.ctypes.data, ctypes.byref(tot)))
+        return offs, crcs, tot.value
+
+    def _read(self, fn, ptr, length: int, max_frames: int | None):
+        cap = length // 16 + 1 if max_frames is None else int(max_frames)
+        cap = min(cap, length // 16 + 1)
+        pay = np.zeros((max(cap, 1), 2), dtype=np.uint64)
+        crcs = np.zeros(max(cap, 1), dtype=np.uint32)
+        status = np.zeros(max(cap, 1), dtype=np.int32)
+        nf = ctypes.c_size_t(0)
+        consumed = ctypes.c_uint64(0)
+        term = ctypes.c_int(0)
+        st = fn(self._h, ptr, length, cap, pay.ctypes.data, crcs.ctypes.data, status.ctypes.data, ctypes.byref(nf),
+                ctypes.byref(consumed), ctypes.byref(term))
+        if st and st not in FRAME_STATUSES:
+            rans.raise_for(st)
+        k = nf.value
+        return pay[:k], crcs[:k], status[:k], consumed.value, bool(term.value)
+
+    def read_blocks(self, d_src, length: int | None = None, max_frames: int | None = None):
+        """Walk the frames of the device tensor d_src[:length]
+        (block.rs:1209-1254, frame after frame) and verify every payload's
+        CRC-32C. Returns (payload spans, crcs, status, consumed, terminated)."""
+        n = d_src.numel() if length is None else int(length)
+        return self._read(self._lib.fqxv_read_blocks, d_src.data_ptr(), n, max_frames)
+
+    def read_blocks_host(self, h_src: np.ndarray, length: int | None = None, max_frames: int | None = None):
+        n = h_src.size if length is None else int(length)
+        return self._read(self._lib.fqxv_read_blocks_host, h_src.ctypes.data, n, max_frames)
+
+    def payload_stream_locs(self, d_src, spans, base: int = 0):
+        """block.rs:961-980 for each plain payload `spans` of d_src: an (n, 3)
+        array of (offset, len, crc) stream locations and per-payload status."""
+        s = _spans(spans)
+        locs = np.zeros((len(s), 3), dtype=STREAM_LOC)
+        status = np.zeros(len(s), dtype=np.int32)
+        st = self._lib.fqxv_payload_stream_locs(self._h, d_src.data_ptr(), s.ctypes.data, len(s), int(base),
+                                                locs.ctypes.data, status.ctypes.data)
+        if st and st not in FRAME_STATUSES:
+            rans.raise_for(st)
+        return locs, status
 
     # ---- per-stage timing ---------------------------------------------------
 

@@ -11,174 +11,10 @@
 
 #include <nvtx3/nvToolsExt.h>
 
-#include "rans_internal.cuh"
+#include "frame_internal.cuh"
+#include "rans_ctx.cuh"
 
 using namespace fqxv;
-
-namespace {
-
-// Grow-only device buffer. Growth waits for the owning stream first, so a
-// buffer is never freed under a kernel that still reads it.
-struct DevBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t want, cudaStream_t s) {
-        if (want <= cap) return cudaSuccess;
-        size_t nc = std::max(want, cap + cap / 2);
-        nc = align_up(nc, 1 << 20);
-        if (p) {
-            cudaStreamSynchronize(s);
-            cudaFree(p);
-            p = nullptr;
-            cap = 0;
-        }
-        cudaError_t e = cudaMalloc(&p, nc);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            e = cudaMalloc(&p, want);
-            if (e != cudaSuccess) {
-                p = nullptr;
-                return e;
-            }
-            nc = want;
-        }
-        cap = nc;
-        return cudaSuccess;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-    template <class T>
-    T *as() const { return reinterpret_cast<T *>(p); }
-};
-
-struct HostBuf {
-    void *p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t want) {
-        if (want <= cap) return cudaSuccess;
-        size_t nc = align_up(std::max(want, cap + cap / 2), 1 << 16);
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-        cudaError_t e = cudaHostAlloc(&p, nc, cudaHostAllocDefault);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return e;
-        }
-        cap = nc;
-        return cudaSuccess;
-    }
-    void release() {
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
-constexpr int kGroups = 6;  // decode launch groups
-
-enum Stage {
-    kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
-    kStDecO1Small, kStages
-};
-const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan", "enc_pack",
-                                          "dec_parse", "dec_o0", "dec_o1_dense", "dec_o1_global",
-                                          "dec_o1_small"};
-
-// CUDA-event brackets around each kernel launch on the context's stream.
-// Durations are collected after the call's final synchronisation.
-struct StageTimer {
-    bool on = false;
-    struct Pending {
-        int stage;
-        cudaEvent_t a, b;
-    };
-    std::vector<Pending> pending;
-    std::vector<cudaEvent_t> pool;
-    double ms[kStages] = {};
-    uint64_t launches[kStages] = {};
-    uint64_t bytes[kStages] = {};   // algorithmic bytes moved by the stage's launches
-    cudaEvent_t get() {
-        if (!pool.empty()) {
-            cudaEvent_t e = pool.back();
-            pool.pop_back();
-            return e;
-        }
-        cudaEvent_t e = nullptr;
-        if (cudaEventCreate(&e) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        return e;
-    }
-    // Returns the start event (or null); pass it to end().
-    cudaEvent_t begin(cudaStream_t s) {
-        if (!on) return nullptr;
-        cudaEvent_t a = get();
-        if (a) cudaEventRecord(a, s);
-        return a;
-    }
-    void end(int stage, cudaEvent_t a, cudaStream_t s) {
-        launches[stage]++;
-        if (!a) return;
-        cudaEvent_t b = get();
-        if (!b) return;
-        cudaEventRecord(b, s);
-        pending.push_back({stage, a, b});
-    }
-    void collect() {
-        for (auto &p : pending) {
-            float t = 0.f;
-            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.stage] += t;
-            else cudaGetLastError();
-            pool.push_back(p.a);
-            pool.push_back(p.b);
-        }
-        pending.clear();
-    }
-    void release() {
-        for (auto &p : pending) {
-            pool.push_back(p.a);
-            pool.push_back(p.b);
-        }
-        pending.clear();
-        for (auto e : pool) cudaEventDestroy(e);
-        pool.clear();
-    }
-};
-
-}  // namespace
-
-struct fqxv_rans_ctx {
-    int device = 0;
-    int sms = 148;
-    cudaStream_t stream = nullptr;
-    cudaStream_t aux[kGroups] = {};   // decode launch groups run side by side
-    cudaEvent_t ev_fork = nullptr, ev_join[kGroups] = {};
-    std::mutex mu;
-    // encode
-    DevBuf e_blocks, e_order, e_jobs, e_tbl, e_words, e_hist, e_misc, e_keys;
-    // decode
-    DevBuf d_streams, d_order, d_tbl, d_misc;
-    // single-call staging
-    DevBuf io_in, io_out;
-    HostBuf h_stage;
-    HostBuf h_io;
-    StageTimer timer;
-    // host-buffer batches cut into chunks run one chunk per sub-context
-    std::vector<fqxv_rans_ctx *> sub;
-    uint64_t device_bytes() const {
-        const DevBuf *all[] = {&e_blocks, &e_order, &e_jobs, &e_tbl, &e_words, &e_hist, &e_misc, &e_keys,
-                               &d_streams, &d_order, &d_tbl, &d_misc, &io_in, &io_out};
-        uint64_t t = 0;
-        for (auto *b : all) t += b->cap;
-        for (auto *c : sub) t += c->device_bytes();
-        return t;
-    }
-};
 
 namespace fqxv {
 int sm_count(int device) {
@@ -188,29 +24,7 @@ int sm_count(int device) {
 }
 }  // namespace fqxv
 
-#define CK(x)                                                          \
-    do {                                                               \
-        cudaError_t e_ = (x);                                          \
-        if (e_ != cudaSuccess) {                                       \
-            cudaGetLastError();                                        \
-            return e_ == cudaErrorMemoryAllocation ? FQXV_RANS_E_OUT_OF_MEMORY \
-                                                   : FQXV_RANS_E_CUDA; \
-        }                                                              \
-    } while (0)
-
 namespace {
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
 
 uint64_t enc_bound_one(uint64_t n, int order) {
     if (n == 0) return kHdr;
@@ -223,9 +37,11 @@ uint64_t enc_bound_one(uint64_t n, int order) {
 constexpr uint64_t kZeroCopyMinBytes = 4ull << 20;
 constexpr size_t kZeroCopyMinStreams = 256;
 
+}  // namespace
+
 // Device address of a pinned, mapped host buffer (nullptr for any other
-// memory): with unified addressing a kernel can load and store it directly.
-void *mapped_device_ptr(const void *h) {
+// memory).
+void *fqxv::mapped_device_ptr(const void *h) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
         cudaGetLastError();
@@ -234,6 +50,8 @@ void *mapped_device_ptr(const void *h) {
     if (a.type != cudaMemoryTypeHost) return nullptr;
     return a.devicePointer;
 }
+
+namespace {
 
 // NVTX range for the lifetime of a scope: the batch calls and their stages
 // show up by name in a timeline profiler (no cost without one attached).
@@ -586,6 +404,11 @@ const char *fqxv_rans_status_message(int status) {
         case FQXV_RANS_E_OUT_OF_MEMORY: return "device out of memory";
         case FQXV_RANS_E_TIMEOUT: return "device wait timed out";
         case FQXV_RANS_E_TOO_LARGE: return "request too large";
+        // crates/fqxv/src/lib.rs:167-178 (the block index is the caller's)
+        case FQXV_FRAME_E_TRUNCATED: return "truncated fqxv stream";
+        case FQXV_FRAME_E_CORRUPT: return "corrupted fqxv data: block (crc mismatch)";
+        case FQXV_FRAME_E_BAD_SYNC: return "corrupted fqxv data: block (bad sync marker) (crc mismatch)";
+        case FQXV_FRAME_E_TOO_LARGE: return "malformed fqxv block: block payload length exceeds the maximum";
         default: return "unknown status";
     }
 }
@@ -629,10 +452,7 @@ void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
     ctx->sub.clear();
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    DevBuf *all[] = {&ctx->e_blocks, &ctx->e_order, &ctx->e_jobs, &ctx->e_tbl, &ctx->e_words,
-                     &ctx->e_hist, &ctx->e_misc, &ctx->e_keys, &ctx->d_streams, &ctx->d_order, &ctx->d_tbl,
-                     &ctx->d_misc, &ctx->io_in, &ctx->io_out};
-    for (auto *b : all) b->release();
+    ctx->for_each_buf([](DevBuf &b) { b.release(); });
     ctx->h_stage.release();
     ctx->h_io.release();
     ctx->timer.release();

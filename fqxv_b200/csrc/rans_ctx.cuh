@@ -1,0 +1,209 @@
+// Device context shared by the C-ABI translation units (rans_capi.cu,
+// frame_capi.cu): arenas, staging buffers, streams and stage timers of one
+// fqxv_rans_ctx. Nothing here is part of the public ABI.
+#pragma once
+
+#include <mutex>
+#include <vector>
+
+#include "rans_internal.cuh"
+
+namespace fqxv {
+
+// Grow-only device buffer. Growth waits for the owning stream first, so a
+// buffer is never freed under a kernel that still reads it.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t want, cudaStream_t s) {
+        if (want <= cap) return cudaSuccess;
+        size_t nc = std::max(want, cap + cap / 2);
+        nc = align_up(nc, 1 << 20);
+        if (p) {
+            cudaStreamSynchronize(s);
+            cudaFree(p);
+            p = nullptr;
+            cap = 0;
+        }
+        cudaError_t e = cudaMalloc(&p, nc);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            e = cudaMalloc(&p, want);
+            if (e != cudaSuccess) {
+                p = nullptr;
+                return e;
+            }
+            nc = want;
+        }
+        cap = nc;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    template <class T>
+    T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t want) {
+        if (want <= cap) return cudaSuccess;
+        size_t nc = align_up(std::max(want, cap + cap / 2), 1 << 16);
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaHostAlloc(&p, nc, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        cap = nc;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+constexpr int kGroups = 6;  // decode launch groups
+
+enum Stage {
+    kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
+    kStDecO1Small, kStCrcPlan, kStCrc, kStFrameCopy, kStFrameWalk, kStages
+};
+const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan", "enc_pack",
+                                          "dec_parse", "dec_o0", "dec_o1_dense", "dec_o1_global",
+                                          "dec_o1_small", "crc_plan", "crc32c", "frame_copy_crc",
+                                          "frame_walk"};
+
+// CUDA-event brackets around each kernel launch on the context's stream.
+// Durations are collected after the call's final synchronisation.
+struct StageTimer {
+    bool on = false;
+    struct Pending {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    double ms[kStages] = {};
+    uint64_t launches[kStages] = {};
+    uint64_t bytes[kStages] = {};   // algorithmic bytes moved by the stage's launches
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return e;
+    }
+    // Returns the start event (or null); pass it to end().
+    cudaEvent_t begin(cudaStream_t s) {
+        if (!on) return nullptr;
+        cudaEvent_t a = get();
+        if (a) cudaEventRecord(a, s);
+        return a;
+    }
+    void end(int stage, cudaEvent_t a, cudaStream_t s) {
+        launches[stage]++;
+        if (!a) return;
+        cudaEvent_t b = get();
+        if (!b) return;
+        cudaEventRecord(b, s);
+        pending.push_back({stage, a, b});
+    }
+    void collect() {
+        for (auto &p : pending) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.stage] += t;
+            else cudaGetLastError();
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void release() {
+        for (auto &p : pending) {
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+        for (auto e : pool) cudaEventDestroy(e);
+        pool.clear();
+    }
+};
+
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Device address of a pinned, mapped host buffer (nullptr for any other
+// memory): with unified addressing a kernel can load and store it directly.
+void *mapped_device_ptr(const void *h);
+
+}  // namespace fqxv
+
+struct fqxv_rans_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaStream_t aux[fqxv::kGroups] = {};   // decode launch groups run side by side
+    cudaEvent_t ev_fork = nullptr, ev_join[fqxv::kGroups] = {};
+    std::mutex mu;
+    // encode
+    fqxv::DevBuf e_blocks, e_order, e_jobs, e_tbl, e_words, e_hist, e_misc, e_keys;
+    // decode
+    fqxv::DevBuf d_streams, d_order, d_tbl, d_misc;
+    // single-call staging
+    fqxv::DevBuf io_in, io_out;
+    // CRC-32C and block frames: targets, pieces, results
+    fqxv::DevBuf f_targets, f_pieces, f_out;
+    fqxv::HostBuf h_stage;
+    fqxv::HostBuf h_io;
+    fqxv::StageTimer timer;
+    // host-buffer batches cut into chunks run one chunk per sub-context
+    std::vector<fqxv_rans_ctx *> sub;
+    template <class F>
+    void for_each_buf(F &&f) {
+        fqxv::DevBuf *all[] = {&e_blocks, &e_order, &e_jobs, &e_tbl, &e_words, &e_hist, &e_misc,
+                               &e_keys, &d_streams, &d_order, &d_tbl, &d_misc, &io_in, &io_out,
+                               &f_targets, &f_pieces, &f_out};
+        for (auto *b : all) f(*b);
+    }
+    uint64_t device_bytes() {
+        uint64_t t = 0;
+        for_each_buf([&](fqxv::DevBuf &b) { t += b.cap; });
+        for (auto *c : sub) t += c->device_bytes();
+        return t;
+    }
+};
+
+#define CK(x)                                                          \
+    do {                                                               \
+        cudaError_t e_ = (x);                                          \
+        if (e_ != cudaSuccess) {                                       \
+            cudaGetLastError();                                        \
+            return e_ == cudaErrorMemoryAllocation ? FQXV_RANS_E_OUT_OF_MEMORY \
+                                                   : FQXV_RANS_E_CUDA; \
+        }                                                              \
+    } while (0)

@@ -125,6 +125,20 @@ def lib() -> ctypes.CDLL:
                                                   ctypes.c_uint64, u8p, u8p]
         L.fqxv_rans_decode_batch_host.argtypes = [ctypes.c_void_p, u8p, u8p, sz, ctypes.c_uint64, u8p, u8p, u8p,
                                                   u8p]
+        # CRC-32C and block frames (include/fqxv_frame_gpu.h)
+        vp = ctypes.c_void_p
+        L.fqxv_crc32c_batch.argtypes = [vp, u8p, u8p, sz, u8p]
+        L.fqxv_crc32c_batch_host.argtypes = [vp, u8p, u8p, sz, u8p]
+        L.fqxv_crc32c_combine.restype = ctypes.c_uint32
+        L.fqxv_crc32c_combine.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
+        L.fqxv_frame_blocks_bound.restype = ctypes.c_uint64
+        L.fqxv_frame_blocks_bound.argtypes = [u8p, sz, ctypes.c_int]
+        L.fqxv_frame_blocks.argtypes = [vp, u8p, u8p, sz, ctypes.c_int, u8p, ctypes.c_uint64, u8p, u8p, u8p]
+        L.fqxv_frame_blocks_host.argtypes = [vp, u8p, u8p, sz, ctypes.c_int, u8p, ctypes.c_uint64, u8p, u8p, u8p]
+        for fn in ("fqxv_read_blocks", "fqxv_read_blocks_host"):
+            getattr(L, fn).argtypes = [vp, u8p, ctypes.c_uint64, sz, u8p, u8p, u8p, szp,
+                                       ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]
+        L.fqxv_payload_stream_locs.argtypes = [vp, u8p, u8p, sz, ctypes.c_uint64, u8p, u8p]
         L.fqxv_rans_ctx_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.fqxv_rans_ctx_stage_stats.argtypes = [ctypes.c_void_p, u8p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.c_int]

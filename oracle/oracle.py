@@ -30,6 +30,10 @@ MESSAGES = {
     8: "truncated renorm stream",
     16: "invalid argument",
     17: "destination buffer too small",
+    32: "truncated fqxv stream",
+    33: "corrupted fqxv data: block (crc mismatch)",
+    34: "corrupted fqxv data: block (bad sync marker) (crc mismatch)",
+    35: "malformed fqxv block: block payload length exceeds the maximum",
 }
 
 
@@ -77,6 +81,20 @@ def lib() -> ctypes.CDLL:
         L.orc_encode_batch.argtypes = [u8p, u64p, u64p, sz, ctypes.c_int, u8p, u64p, u64p, u64p, i32p,
                                        ctypes.c_int]
         L.orc_decode_batch.argtypes = [u8p, u64p, u64p, sz, u8p, u64p, u64p, u64p, i32p, ctypes.c_int]
+        # CRC-32C and block frames (frame_oracle.c)
+        L.orc_crc32c.restype = ctypes.c_uint32
+        L.orc_crc32c.argtypes = [u8p, sz]
+        L.orc_crc32c_update.restype = ctypes.c_uint32
+        L.orc_crc32c_update.argtypes = [ctypes.c_uint32, u8p, sz]
+        L.orc_crc32c_combine.restype = ctypes.c_uint32
+        L.orc_crc32c_combine.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
+        L.orc_frame_blocks.argtypes = [u8p, u64p, u64p, sz, ctypes.c_int, u8p, ctypes.c_uint64, u64p,
+                                       ctypes.POINTER(ctypes.c_uint32), u64p]
+        L.orc_read_blocks.argtypes = [u8p, ctypes.c_uint64, sz, u64p, u64p, ctypes.POINTER(ctypes.c_uint32), i32p,
+                                      szp, u64p, ctypes.POINTER(ctypes.c_int)]
+        L.orc_crc32c_batch.argtypes = [u8p, u64p, u64p, sz, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int]
+        L.orc_payload_stream_locs.argtypes = [u8p, ctypes.c_uint64, ctypes.c_uint64, u64p,
+                                              ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
         _lib = L
     return _lib
 
@@ -214,3 +232,77 @@ def decode_batch(src: np.ndarray, offs: np.ndarray, lens: np.ndarray, out_lens: 
     if rc:
         raise OracleError(rc)
     return dst, doff, ol
+
+
+# ---- CRC-32C and block frames (frame_oracle.c) --------------------------------
+
+def crc32c(data) -> int:
+    """crates/fqxv/src/crc.rs:74."""
+    a, p = _buf(data)
+    return int(lib().orc_crc32c(p, a.size))
+
+
+def crc32c_combine(crc_a: int, crc_b: int, len_b: int) -> int:
+    """crc.rs:116."""
+    return int(lib().orc_crc32c_combine(crc_a, crc_b, len_b))
+
+
+def frame_blocks(src: np.ndarray, offs, lens, terminate: bool = False):
+    """crates/fqxv/src/container/block.rs:110-142 over payloads of `src`.
+    Returns (frames bytes, frame offsets, crcs)."""
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    n = len(offs)
+    need = int(lens.sum()) + 16 * n + (12 if terminate else 0)
+    dst = np.zeros(max(need, 1), dtype=np.uint8)
+    fo = np.zeros(max(n, 1), dtype=np.uint64)
+    crcs = np.zeros(max(n, 1), dtype=np.uint32)
+    tot = ctypes.c_uint64(0)
+    src = np.ascontiguousarray(src, dtype=np.uint8)
+    rc = lib().orc_frame_blocks(_ptr(src, ctypes.c_uint8), _ptr(offs, ctypes.c_uint64), _ptr(lens, ctypes.c_uint64),
+                                n, 1 if terminate else 0, _ptr(dst, ctypes.c_uint8), need,
+                                _ptr(fo, ctypes.c_uint64), _ptr(crcs, ctypes.c_uint32), ctypes.byref(tot))
+    if rc:
+        raise OracleError(rc)
+    return dst[:need].tobytes(), fo[:n], crcs[:n]
+
+
+def read_blocks(buf, max_frames: int | None = None):
+    """block.rs:1209-1254 frame after frame. Returns (first status, payload
+    spans (k, 2), crcs, status, consumed, terminated)."""
+    a, p = _buf(buf)
+    cap = a.size // 16 + 1 if max_frames is None else min(int(max_frames), a.size // 16 + 1)
+    po = np.zeros(max(cap, 1), dtype=np.uint64)
+    pl = np.zeros(max(cap, 1), dtype=np.uint64)
+    crcs = np.zeros(max(cap, 1), dtype=np.uint32)
+    st = np.zeros(max(cap, 1), dtype=np.int32)
+    nf = ctypes.c_size_t(0)
+    consumed = ctypes.c_uint64(0)
+    term = ctypes.c_int(0)
+    first = lib().orc_read_blocks(p, a.size, cap, _ptr(po, ctypes.c_uint64), _ptr(pl, ctypes.c_uint64),
+                                  _ptr(crcs, ctypes.c_uint32), _ptr(st, ctypes.c_int32), ctypes.byref(nf),
+                                  ctypes.byref(consumed), ctypes.byref(term))
+    k = nf.value
+    return first, np.stack([po[:k], pl[:k]], axis=1), crcs[:k], st[:k], consumed.value, bool(term.value)
+
+
+def payload_stream_locs(payload, block_offset: int):
+    """block.rs:961-980. Returns (status, [(offset, len, crc)] x 3)."""
+    a, p = _buf(payload)
+    off = np.zeros(3, dtype=np.uint64)
+    ln = np.zeros(3, dtype=np.uint32)
+    crc = np.zeros(3, dtype=np.uint32)
+    rc = lib().orc_payload_stream_locs(p, a.size, block_offset, _ptr(off, ctypes.c_uint64),
+                                       _ptr(ln, ctypes.c_uint32), _ptr(crc, ctypes.c_uint32))
+    return rc, [(int(off[i]), int(ln[i]), int(crc[i])) for i in range(3)]
+
+
+def crc32c_batch(src: np.ndarray, offs, lens, nthreads: int = 0) -> np.ndarray:
+    """CRC-32C of many spans of `src` on host threads (the CPU baseline)."""
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    out = np.zeros(max(len(offs), 1), dtype=np.uint32)
+    src = np.ascontiguousarray(src, dtype=np.uint8)
+    lib().orc_crc32c_batch(_ptr(src, ctypes.c_uint8), _ptr(offs, ctypes.c_uint64), _ptr(lens, ctypes.c_uint64),
+                           len(offs), _ptr(out, ctypes.c_uint32), nthreads)
+    return out[:len(offs)]

@@ -39,7 +39,12 @@ enum {
     ORC_E_BOUND = 7,             /* "rANS output length exceeds caller bound" lib.rs:228 */
     ORC_E_TRUNCATED_RENORM = 8,  /* "truncated renorm stream"           avx2.rs:207 */
     ORC_E_INVALID_ARG = 16,
-    ORC_E_DST_TOO_SMALL = 17
+    ORC_E_DST_TOO_SMALL = 17,
+    /* container frames (crates/fqxv/src/lib.rs:167-178, block.rs:1209-1254) */
+    ORC_FRAME_E_TRUNCATED = 32,  /* Error::Truncated "truncated fqxv stream" */
+    ORC_FRAME_E_CORRUPT = 33,    /* Error::Corrupt "block {i}" (crc mismatch) */
+    ORC_FRAME_E_BAD_SYNC = 34,   /* Error::Corrupt "block {i} (bad sync marker)" */
+    ORC_FRAME_E_TOO_LARGE = 35   /* Error::Malformed("block payload length exceeds the maximum") */
 };
 
 /* model.rs:9-19 */
@@ -113,6 +118,23 @@ int orc_encode_batch(const uint8_t *src, const uint64_t *src_off, const uint64_t
 int orc_decode_batch(const uint8_t *src, const uint64_t *src_off, const uint64_t *src_len,
                      size_t nblocks, uint8_t *dst, const uint64_t *dst_off,
                      const uint64_t *dst_cap, uint64_t *out_len, int32_t *status, int nthreads);
+
+/* ---- CRC-32C and block frames (frame_oracle.c) ------------------------
+ * crates/fqxv/src/crc.rs and crates/fqxv/src/container/block.rs. */
+#define ORC_FRAME_HEAD 16u                     /* format.rs:99 FRAME_HEAD_LEN */
+#define ORC_FRAME_TERM 12u                     /* "FQXB" + u64 0 */
+#define ORC_MAX_BLOCK_PAYLOAD (1ull << 31)     /* format.rs:87 (256 MiB x 8) */
+uint32_t orc_crc32c(const uint8_t *p, size_t n);
+uint32_t orc_crc32c_update(uint32_t state, const uint8_t *p, size_t n);
+uint32_t orc_crc32c_combine(uint32_t crc_a, uint32_t crc_b, uint64_t len_b);
+int orc_frame_blocks(const uint8_t *src, const uint64_t *off, const uint64_t *len, size_t n, int terminate,
+                     uint8_t *dst, uint64_t cap, uint64_t *frame_off, uint32_t *crcs, uint64_t *total);
+int orc_read_blocks(const uint8_t *src, uint64_t len, size_t max_frames, uint64_t *pay_off, uint64_t *pay_len,
+                    uint32_t *crcs, int32_t *status, size_t *nframes, uint64_t *consumed, int *terminated);
+int orc_crc32c_batch(const uint8_t *src, const uint64_t *off, const uint64_t *len, size_t n, uint32_t *out,
+                     int nthreads);
+int orc_payload_stream_locs(const uint8_t *payload, uint64_t len, uint64_t block_offset, uint64_t loc_off[3],
+                            uint32_t loc_len[3], uint32_t loc_crc[3]);
 
 #ifdef __cplusplus
 }

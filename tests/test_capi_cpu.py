@@ -17,14 +17,16 @@ def _declared():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        names |= set(re.findall(r"\b(fqxv_rans_\w+)\s*\(", text))
+        names |= set(re.findall(r"\b(fqxv_\w+)\s*\(", text))
     return sorted(names)
 
 
 def test_header_declares_the_reference_api():
     names = _declared()
     for fn in ["fqxv_rans_encode", "fqxv_rans_decode", "fqxv_rans_decode_bounded", "fqxv_rans_decode_with",
-               "fqxv_rans_peek_output_len", "fqxv_rans_encode_batch", "fqxv_rans_decode_batch"]:
+               "fqxv_rans_peek_output_len", "fqxv_rans_encode_batch", "fqxv_rans_decode_batch",
+               "fqxv_crc32c_batch", "fqxv_crc32c_combine", "fqxv_frame_blocks", "fqxv_read_blocks",
+               "fqxv_payload_stream_locs"]:
         assert fn in names
 
 
