@@ -20,8 +20,6 @@ constexpr uint64_t kMaxBlockPayload = 1ull << 31;    // MAX_BLOCK_SEQ_BYTES (256
 constexpr int kCrcThreads = 1024;
 constexpr int kCrcUnroll = 8;
 constexpr int kCopyUnroll = 4;
-// Lines (128 bytes) a warp's L2 bulk prefetch runs ahead of its loads.
-constexpr uint32_t kPrefetchLines = 64;
 // Piece size 2^shift: about kCrcPieceTarget pieces per pass (four per warp
 // slot of 148 SMs x 32 warps), between 32 KiB and 256 KiB.
 constexpr int kCrcMinShift = 15;

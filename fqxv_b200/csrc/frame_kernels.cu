@@ -141,18 +141,6 @@ __device__ __forceinline__ uint32_t mask_word(uint32_t w, uint64_t y, uint64_t l
 
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t *p) { return __ldcs(p); }
 
-// Bulk prefetch of the bytes [a, b) into L2 by the copy engine (no
-// registers held while the lines are in flight). The range is widened to
-// whole 16-byte blocks, which hold bytes of the range, so it stays inside
-// the allocation.
-__device__ __forceinline__ void prefetch_l2(uint64_t a, uint64_t b) {
-    if (b <= a) return;
-    const uint64_t lo = a & ~15ull;
-    const uint64_t hi = (b + 15) & ~15ull;
-    const uint32_t n = (uint32_t)(hi - lo);
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"(n) : "memory");
-}
-
 // The 4-byte word at aligned source address a, or 0 when it holds no byte of
 // the source range [lo, hi) (so nothing outside the range is ever read).
 __device__ __forceinline__ uint32_t ld_guard(uint64_t a, uint64_t lo, uint64_t hi) {
@@ -169,8 +157,6 @@ __device__ __forceinline__ void st_masked(uint32_t w, uint64_t y, uint64_t lo, u
     for (int b = 0; b < 4; b++)
         if (y + b >= lo && y + b < hi) *reinterpret_cast<uint8_t *>(y + b) = (uint8_t)(w >> (8 * b));
 }
-
-__device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
 struct LaneTables {
     const uint32_t *g;  // this lane's column of the Z^128 byte tables
@@ -273,11 +259,6 @@ __global__ void __launch_bounds__(kCrcThreads, 1)
             return w;
         };
 
-        // The copy engine streams the piece into L2 kPrefetchLines ahead of
-        // the lines being loaded (source bytes: the lines' as0 grid for a copy).
-        const uint64_t pf0 = COPY ? as0 - 4 * lane : Ya;  // lane 0's word of line 0
-        const uint64_t pf_end = COPY ? shi : hi;
-        if (lane == 0) prefetch_l2(COPY ? slo : lo, min_u64(pf0 + 128ull * kPrefetchLines, pf_end));
         uint32_t s = 0;
         {
             const uint32_t x = word(0, true);
@@ -294,10 +275,6 @@ __global__ void __launch_bounds__(kCrcThreads, 1)
         const bool extra = COPY && sh && lane == 31;
         uint32_t wa[U], wb[U], xa = 0, xb = 0;
         auto load = [&](uint32_t *w, uint32_t &xl, uint32_t mm) {
-            if (lane == 0) {
-                const uint64_t a = pf0 + 128ull * (mm + kPrefetchLines);
-                prefetch_l2(a, min_u64(a + 128ull * U, pf_end));
-            }
 #pragma unroll
             for (int j = 0; j < U; j++) w[j] = ld_stream(q + 32 * (mm + j));
             if (extra) xl = ld_stream(q + 32 * (mm + U - 1) + 1);
@@ -741,9 +718,13 @@ __global__ void __launch_bounds__(1024, 1)
     const uint32_t hi = lo + per < n ? lo + per : n;
     unsigned long long t = 0;
     for (uint32_t i = lo; i < hi; i++) t += targets[i].len;
-    if (tid == 0) s_total = 0;
+    s_sum[tid] = t;
     __syncthreads();
-    atomicAdd(&s_total, t);
+    for (uint32_t o = nth >> 1; o; o >>= 1) {  // total (nth is a power of two)
+        if (tid < o) s_sum[tid] += s_sum[tid + o];
+        __syncthreads();
+    }
+    if (tid == 0) s_total = s_sum[0];
     __syncthreads();
     const int psh = crc_piece_shift(s_total, kCrcPieceTarget, kCrcMinShift, kCrcMaxShift);
     unsigned long long c = 0;
