@@ -158,27 +158,43 @@ __device__ __forceinline__ void st_masked(uint32_t w, uint64_t y, uint64_t lo, u
         if (y + b >= lo && y + b < hi) *reinterpret_cast<uint8_t *>(y + b) = (uint8_t)(w >> (8 * b));
 }
 
+// Shared memory: the four Z^128 byte tables, replicated once per lane, then
+// the Z^r multipliers. Entry b of table k for lane l sits at byte
+//   (k & 1) * 64 KiB + b * 256 + (k >> 1) * 128 + l * 4,
+// so a warp's 32 lookups hit 32 banks, and the address of a lookup is one
+// byte permute: [l * 4, byte k of x, 0, 0] plus an immediate table base.
+constexpr uint32_t kTabWords = 4 * 256 * 32;
+constexpr uint32_t kPieceSmem = (kTabWords + kZMax) * 4;
+
 struct LaneTables {
-    const uint32_t *g;  // this lane's column of the Z^128 byte tables
+    const uint8_t *base;  // shared memory base of the tables
+    uint32_t lane4;       // l * 4
+    __device__ __forceinline__ uint32_t at(uint32_t off) const {
+        return *reinterpret_cast<const uint32_t *>(base + off);
+    }
     __device__ __forceinline__ uint32_t step(uint32_t x) const {
-        return g[(x & 0xFFu) << 5] ^ g[(256u + ((x >> 8) & 0xFFu)) << 5] ^
-               g[(512u + ((x >> 16) & 0xFFu)) << 5] ^ g[(768u + (x >> 24)) << 5];
+        const uint32_t a0 = __byte_perm(x, lane4, 0x5504);  // byte 0 of x
+        const uint32_t a1 = __byte_perm(x, lane4, 0x5514);
+        const uint32_t a2 = __byte_perm(x, lane4, 0x5524);
+        const uint32_t a3 = __byte_perm(x, lane4, 0x5534);
+        return at(a0) ^ at(a1 + 65536u) ^ at(a2 + 128u) ^ at(a3 + 65536u + 128u);
     }
 };
 
-// Shared memory: [4][256][32] u32 lane-replicated Z^128 tables (128 KiB),
-// then the Z^r multipliers.
-constexpr uint32_t kTabWords = 4 * 256 * 32;
-constexpr uint32_t kPieceSmem = (kTabWords + kZMax) * 4;
+__device__ __forceinline__ uint32_t tab_offset(uint32_t k, uint32_t b, uint32_t lane) {
+    return (k & 1u) * 65536u + b * 256u + (k >> 1) * 128u + lane * 4u;
+}
 
 __device__ void build_tables(uint32_t *smem) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // entry e = 256 k + b of table k: (b << 8k) * x^(8 * 128)
     const uint32_t e = threadIdx.x;
     const uint32_t v = gf_mul((e & 0xFFu) << (8 * (e >> 8)), c_crc.z[128]);
+    uint8_t *sb = reinterpret_cast<uint8_t *>(smem);
     for (int j = 0; j < 32; j++) {
         const uint32_t x = __shfl_sync(0xFFFFFFFFu, v, j);
-        smem[((warp << 5) + j) * 32 + lane] = x;
+        const uint32_t ej = (warp << 5) + j;
+        *reinterpret_cast<uint32_t *>(sb + tab_offset(ej >> 8, ej & 0xFFu, lane)) = x;
     }
     for (uint32_t i = threadIdx.x; i < kZMax; i += blockDim.x) smem[kTabWords + i] = c_crc.z[i];
 }
@@ -208,7 +224,7 @@ __global__ void __launch_bounds__(kCrcThreads, 1)
     build_tables(smem);
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const LaneTables G{smem + lane};
+    const LaneTables G{reinterpret_cast<const uint8_t *>(smem), 4u * lane};
     const uint32_t *sZ = smem + kTabWords;
     const uint32_t npieces = job->npieces;
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
