@@ -18,7 +18,7 @@ constexpr uint64_t kMaxBlockPayload = 1ull << 31;    // MAX_BLOCK_SEQ_BYTES (256
 // 2 x kCrcUnroll lines of loads in flight (2 x kCopyUnroll for the frame
 // copy, which also holds the realigned words and moves twice the bytes).
 constexpr int kCrcThreads = 1024;
-constexpr int kCrcUnroll = 8;
+constexpr int kCrcUnroll = 12;
 constexpr int kCopyUnroll = 4;
 // Piece size 2^shift: about kCrcPieceTarget pieces per pass (four per warp
 // slot of 148 SMs x 32 warps), between 32 KiB and 256 KiB.
