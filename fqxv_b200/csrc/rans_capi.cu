@@ -11,6 +11,7 @@
 
 #include <nvtx3/nvToolsExt.h>
 
+#include "../../include/fqxv_tok_gpu.h"
 #include "frame_internal.cuh"
 #include "rans_ctx.cuh"
 
@@ -409,6 +410,21 @@ const char *fqxv_rans_status_message(int status) {
         case FQXV_FRAME_E_CORRUPT: return "corrupted fqxv data: block (crc mismatch)";
         case FQXV_FRAME_E_BAD_SYNC: return "corrupted fqxv data: block (bad sync marker) (crc mismatch)";
         case FQXV_FRAME_E_TOO_LARGE: return "malformed fqxv block: block payload length exceeds the maximum";
+        // crates/fqxv-tokenizer/src/lib.rs Error::Malformed texts
+        case FQXV_TOK_E_VERSION: return "malformed name stream: unsupported version";
+        case FQXV_TOK_E_TRUNCATED: return "malformed name stream: truncated";
+        case FQXV_TOK_E_VARINT: return "malformed name stream: varint too long";
+        case FQXV_TOK_E_RECORDS: return "malformed name stream: record count exceeds token stream";
+        case FQXV_TOK_E_SYM_UNDERRUN: return "malformed name stream: op sym underrun";
+        case FQXV_TOK_E_RUN_TOO_LONG: return "malformed name stream: op run too long";
+        case FQXV_TOK_E_OPS_BOUND: return "malformed name stream: op columns exceed the stream bound";
+        case FQXV_TOK_E_PLANE_LEN: return "malformed name stream: delta plane length mismatch";
+        case FQXV_TOK_E_MATCH: return "malformed name stream: MATCH without prior token";
+        case FQXV_TOK_E_STR_UNDERRUN: return "malformed name stream: string data underrun";
+        case FQXV_TOK_E_PAD_UNDERRUN: return "malformed name stream: pad underrun";
+        case FQXV_TOK_E_DELTA_UNDERRUN: return "malformed name stream: delta underrun";
+        case FQXV_TOK_E_DELTA_PRIOR: return "malformed name stream: DELTA without numeric prior";
+        case FQXV_TOK_E_UNKNOWN_OP: return "malformed name stream: unknown op";
         default: return "unknown status";
     }
 }

@@ -139,6 +139,11 @@ def lib() -> ctypes.CDLL:
             getattr(L, fn).argtypes = [vp, u8p, ctypes.c_uint64, sz, u8p, u8p, u8p, szp,
                                        ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)]
         L.fqxv_payload_stream_locs.argtypes = [vp, u8p, u8p, sz, ctypes.c_uint64, u8p, u8p]
+        # read-name tokenizer (include/fqxv_tok_gpu.h)
+        L.fqxv_tok_encode_host.argtypes = [vp, u8p, u8p, sz, u8p, sz, u8p, ctypes.c_uint64, u8p,
+                                           ctypes.POINTER(ctypes.c_uint64)]
+        L.fqxv_tok_decode_host.argtypes = [vp, u8p, u8p, sz, u8p, ctypes.c_uint64, u8p, ctypes.c_uint64, u8p, u8p,
+                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
         L.fqxv_rans_ctx_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.fqxv_rans_ctx_stage_stats.argtypes = [ctypes.c_void_p, u8p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.c_int]
