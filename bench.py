@@ -20,6 +20,8 @@ Workloads (seeded synthetic data of the benchmark shapes):
            full-range order-1: peak batched throughput of one order
   cpu_single (with --impl reference)  the CPU coder on one thread, 8 MiB of
            quality_like data, per path (the reference's own benchmark shape)
+  names    read-name tokenizer (crates/fqxv-tokenizer): 256 blocks x 4000
+           Illumina-style names, encode then decode through the C ABI
   crc      CRC-32C of 4096 payloads 4 KiB - 4 MiB (crates/fqxv/src/crc.rs)
   frame    block frames of the same payloads: write (copy + CRC-32C, terminator)
            then read back with every CRC verified (container/block.rs)
@@ -310,6 +312,198 @@ def run_frames_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+NAMES_METRIC = "read-name tokenizer encode + decode GB/s, byte-identical (name bytes per second)"
+
+
+def names_workload(seed: int, blocks: int = 0):
+    """Illumina-style read names `A00123:8:H7KJ2DSXX:<lane>:<tile>:<x>:<y>`, 4000
+    per block (the container's block size range), tiles advancing, x / y
+    uniform; half the blocks carry the paired-read comment ` 1:N:0:<index>`."""
+    nb = blocks or 256
+    rng = np.random.default_rng(2000 + seed)
+    names, bspans = [], []
+    for b in range(nb):
+        x = rng.integers(1000, 32000, 4000)
+        y = rng.integers(1000, 32000, 4000)
+        tile = 1101 + (np.arange(4000) + int(rng.integers(0, 400))) // 400
+        suffix = b" 1:N:0:ATCACG" if b % 2 else b""
+        first = len(names)
+        names += [b"A00123:8:H7KJ2DSXX:%d:%d:%d:%d%s" % (1 + b % 4, tile[i], x[i], y[i], suffix)
+                  for i in range(4000)]
+        bspans.append((first, 4000))
+    lens = np.array([len(n) for n in names], dtype=np.uint64)
+    offs = np.zeros(len(names), dtype=np.uint64)
+    offs[1:] = np.cumsum(lens)[:-1]
+    arena = np.frombuffer(b"".join(names), dtype=np.uint8).copy()
+    return (arena, np.ascontiguousarray(np.stack([offs, lens], 1)), np.array(bspans, dtype=np.uint64),
+            "%d blocks x 4000 Illumina-style names" % nb)
+
+
+class NamesCoder:
+    """fqxv_tok_encode_host + fqxv_tok_decode_host over one library (the GPU
+    library, or the CPU build of the same host code over the oracle coder)."""
+
+    def __init__(self, lib, ctx, arena, nspans, bspans):
+        import ctypes
+
+        self.L, self.ctx, self.arena, self.nspans, self.bspans = lib, ctx, arena, nspans, bspans
+        vp, sz, u64p = ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)
+        lib.fqxv_tok_encode_host.argtypes = [vp, vp, vp, sz, vp, sz, vp, ctypes.c_uint64, vp, u64p]
+        lib.fqxv_tok_decode_host.argtypes = [vp, vp, vp, sz, vp, ctypes.c_uint64, vp, ctypes.c_uint64, vp, vp,
+                                             u64p, u64p]
+        self.nb = len(bspans)
+        self.pay = np.zeros(arena.size + 8192 * self.nb, dtype=np.uint8)
+        self.pspans = np.zeros((self.nb, 2), dtype=np.uint64)
+        self.names = np.zeros(arena.size, dtype=np.uint8)
+        self.out_nspans = np.zeros((len(nspans), 2), dtype=np.uint64)
+        self.out_b = np.zeros((self.nb, 2), dtype=np.uint64)
+        self.status = np.zeros(self.nb, dtype=np.int32)
+        self.c = ctypes
+
+    def encode(self):
+        need = self.c.c_uint64(0)
+        st = self.L.fqxv_tok_encode_host(self.ctx, self.arena.ctypes.data, self.nspans.ctypes.data, len(self.nspans),
+                                         self.bspans.ctypes.data, self.nb, self.pay.ctypes.data, self.pay.size,
+                                         self.pspans.ctypes.data, self.c.byref(need))
+        assert st == 0, st
+        return int(need.value)
+
+    def decode(self):
+        a, b = self.c.c_uint64(0), self.c.c_uint64(0)
+        st = self.L.fqxv_tok_decode_host(self.ctx, self.pay.ctypes.data, self.pspans.ctypes.data, self.nb,
+                                         self.names.ctypes.data, self.names.size, self.out_nspans.ctypes.data,
+                                         len(self.out_nspans), self.out_b.ctypes.data, self.status.ctypes.data,
+                                         self.c.byref(a), self.c.byref(b))
+        assert st == 0 and not self.status.any(), st
+
+    def check(self):
+        assert np.array_equal(self.names, self.arena) and np.array_equal(self.out_nspans, self.nspans)
+
+
+def names_cpu_rate(arena, nspans, bspans, k: int):
+    """The CPU build of the tokenizer host code over the oracle coder, all host
+    threads, on the first k blocks: (GB/s, reps, bytes, threads)."""
+    import ctypes
+
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "libtok_cpu.so"))
+    sub_b = bspans[:k]
+    n_names = int(sub_b[-1, 0] + sub_b[-1, 1])
+    sub_n = nspans[:n_names]
+    nbytes = int(sub_n[-1, 0] + sub_n[-1, 1])
+    coder = NamesCoder(L, ctypes.c_void_p(1), arena[:nbytes].copy(), sub_n.copy(), sub_b.copy())
+    coder.encode()
+    coder.decode()
+    coder.check()
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < 10.0 and reps < 20:
+        coder.encode()
+        coder.decode()
+        reps += 1
+    dt = time.perf_counter() - t0
+    return nbytes * reps / dt / 1e9, reps, nbytes, os.cpu_count() or 1
+
+
+def run_names(args, rank: int, world: int, local: int, dist) -> None:
+    import torch
+
+    from fqxv_b200 import frame, rans
+
+    arena, nspans, bspans, desc = names_workload(args.seed + rank, args.blocks)
+    n_bytes = int(arena.size)
+    codec = frame.codec(local)
+    coder = NamesCoder(rans.lib(), codec._h, arena, nspans, bspans)
+    for _ in range(args.warmup):
+        payload_bytes = coder.encode()
+        coder.decode()
+    coder.check()
+    codec.stage_stats(reset=True)
+    codec.set_profiling(True)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    enc_s = dec_s = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        coder.encode()
+        t1 = time.perf_counter()
+        coder.decode()
+        t2 = time.perf_counter()
+        enc_s += t1 - t0
+        dec_s += t2 - t1
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    codec.set_profiling(False)
+    stages = codec.stage_stats(reset=True)
+    total_s = enc_s + dec_s
+    t = torch.tensor([total_s, enc_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_s, enc_s = float(t[0]), float(t[1])
+    value = world * n_bytes * args.steps / total_s / 1e9
+    pk = peaks()
+    timed = {k: v for k, v in stages.items() if v["launches"] > 0}
+    dom = max(timed, key=lambda k: timed[k]["ms"])
+    per_launch_ms = timed[dom]["ms"] / timed[dom]["launches"]
+    alg_bytes = timed[dom]["bytes"] / timed[dom]["launches"]
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
+    gpu_ms = sum(v["ms"] for v in timed.values()) / args.steps
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 6), "traffic": None,
+                "alg_bytes_per_launch": int(alg_bytes), "launch_ms": round(per_launch_ms, 4),
+                "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"}
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        rate, reps, nb_s, thr = names_cpu_rate(arena, nspans, bspans, min(32, len(bspans)))
+        cpu = {"value": round(rate, 4), "unit": "GB/s", "cores": thr, "kind": "port",
+               "sample": "%d encode + decode passes over the first 32 blocks (%d name bytes): the tokenizer host "
+                         "code over the C restatement of the fqxv-rans CPU coder (both orders, keep the smaller), "
+                         "streams spread over %d host threads" % (reps, nb_s, thr)}
+    if rank == 0:
+        line = {
+            "metric": NAMES_METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "names", "desc": desc, "blocks": int(len(bspans)), "names": int(len(nspans)),
+                       "bytes_per_gpu": n_bytes, "payload_bytes_per_gpu": payload_bytes,
+                       "timing": "host clock around the synchronous C-ABI calls (host buffers in and out), so "
+                                 "value is end to end; GPU kernel time per step in gpu_ms_per_step",
+                       "l2": "inputs come from host memory every step",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "encode_gbs": round(world * n_bytes * args.steps / enc_s / 1e9, 4),
+            "decode_gbs": round(world * n_bytes * args.steps / (total_s - enc_s) / 1e9, 4),
+            "gpu_ms_per_step": round(gpu_ms, 3),
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": n_bytes + payload_bytes,
+                    "d2h_bytes_per_step": n_bytes + payload_bytes,
+                    "path": "fqxv_tok_encode_host + fqxv_tok_decode_host (host buffers)"},
+            "gpu_launches": int(sum(v["launches"] for v in stages.values())),
+            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "bytes": v["bytes"]}
+                       for k, v in stages.items() if v["launches"]},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_names_reference(args) -> None:
+    arena, nspans, bspans, desc = names_workload(args.seed, args.blocks)
+    rate, reps, nb_s, thr = names_cpu_rate(arena, nspans, bspans, min(32, len(bspans)))
+    line = {"impl": "reference", "metric": NAMES_METRIC, "value": round(rate, 4), "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": reps, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "names", "desc": desc, "timed_sample_bytes": nb_s},
+            "cpu_baseline": {"value": round(rate, 4), "unit": "GB/s", "cores": thr, "kind": "port",
+                             "sample": "the first 32 blocks: tokenizer host code over the C restatement of the "
+                                       "fqxv-rans CPU coder on all host threads"},
+            "e2e": {"value": round(rate, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -497,6 +691,9 @@ def run_reference(args, rank: int) -> None:
     if args.workload in FRAME_METRICS:
         run_frames_reference(args)
         return
+    if args.workload == "names":
+        run_names_reference(args)
+        return
     data, spans, order, desc, extra = build_workload(args.workload, args.seed, args.blocks)
     nthreads = os.cpu_count() or 1
     n_bytes = int(spans[:, 1].sum())
@@ -668,7 +865,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config1",
                     choices=["config1", "config0", "config2", "config3", "config4", "batch0", "batch1", "batch1f",
-                             "cpu_single", "crc", "frame"])
+                             "cpu_single", "crc", "frame", "names"])
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
     ap.add_argument("--workers", type=int, default=8, help="config4: server workers (streams)")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
@@ -707,8 +904,8 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    if args.workload in FRAME_METRICS:
-        run_frames(args, rank, world, local, dist)
+    if args.workload in FRAME_METRICS or args.workload == "names":
+        (run_names if args.workload == "names" else run_frames)(args, rank, world, local, dist)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

@@ -323,25 +323,37 @@ struct DecodeList {
     const uint8_t *data(const std::vector<uint8_t> &dst, size_t k) const { return dst.data() + out[gpu_index[k]].offset; }
 };
 
-struct DTok {
-    bool is_num;
-    std::string bytes;
-    int64_t value;
-};
-
-DTok num_tok(int64_t value, size_t width) {  // lib.rs:684-699
-    std::string s = std::to_string(value);
-    if (s.size() < width) s = std::string(width - s.size(), '0') + s;
-    return DTok{true, std::move(s), value};
-}
-
 struct BlockOut {
     int status = FQXV_RANS_OK;
     std::vector<uint8_t> bytes;
     std::vector<uint64_t> name_len;
 };
 
-// lib.rs:580-650: names from the decoded role streams.
+// A rebuilt token: its bytes are in the block's output at [off, off + len).
+struct OTok {
+    uint64_t off;
+    uint32_t len;
+    bool is_num;
+    int64_t value;
+};
+
+// lib.rs:684-699 num_tok: the decimal value, zero-padded on the left to
+// `width`, appended to `out`.
+void put_num(std::vector<uint8_t> &out, int64_t value, size_t width) {
+    char buf[24];
+    int n = 0;
+    uint64_t m = value < 0 ? 0 - (uint64_t)value : (uint64_t)value;
+    do {
+        buf[n++] = (char)('0' + m % 10);
+        m /= 10;
+    } while (m);
+    if (value < 0) buf[n++] = '-';
+    for (size_t k = (size_t)n; k < width; k++) out.push_back('0');
+    while (n) out.push_back((uint8_t)buf[--n]);
+}
+
+// lib.rs:580-650: names from the decoded role streams, written straight into
+// the block's output (a MATCH copies the previous name's token).
 int rebuild_names(uint64_t n_records, const uint8_t *counts, uint64_t ncounts, const uint8_t *str_lens,
                   uint64_t nsl, const uint8_t *str_data, uint64_t nsd, const uint8_t *num_vals, uint64_t nnv,
                   const uint8_t *pads, uint64_t npads, const std::vector<std::vector<uint8_t>> &ops,
@@ -351,50 +363,54 @@ int rebuild_names(uint64_t n_records, const uint8_t *counts, uint64_t ncounts, c
     std::vector<size_t> dpos(kCols, 0);
     Reader cc{counts, ncounts}, cl{str_lens, nsl}, cn{num_vals, nnv};
     uint64_t str_pos = 0, pad_pos = 0;
-    std::vector<DTok> prev, cur;
+    std::vector<OTok> prev, cur;
+    std::vector<uint8_t> &ob = out.bytes;
+    ob.reserve(nsd + 32 * n_records);
+    out.name_len.reserve(n_records);
     int e;
     for (uint64_t rec = 0; rec < n_records; rec++) {
         uint64_t nt = 0;
         if ((e = cc.varint(nt))) return e;
         cur.clear();
+        const uint64_t name_start = ob.size();
         for (uint64_t t = 0; t < nt; t++) {
             const size_t col = std::min<size_t>(cur.size(), kCols - 1);
             uint8_t o = 0;
             if ((e = op[col].u8(o))) return e;
+            const uint64_t at = ob.size();
             if (o == kMatch) {
                 if (cur.size() >= prev.size()) return FQXV_TOK_E_MATCH;
-                cur.push_back(prev[cur.size()]);
+                const OTok p = prev[cur.size()];
+                ob.resize(at + p.len);
+                std::memcpy(ob.data() + at, ob.data() + p.off, p.len);
+                cur.push_back(OTok{at, p.len, p.is_num, p.value});
             } else if (o == kStr) {
                 uint64_t l = 0;
                 if ((e = cl.varint(l))) return e;
                 if (l > nsd || str_pos > nsd - l) return FQXV_TOK_E_STR_UNDERRUN;
-                cur.push_back(DTok{false, std::string((const char *)str_data + str_pos, l), 0});
+                ob.insert(ob.end(), str_data + str_pos, str_data + str_pos + l);
                 str_pos += l;
-            } else if (o == kNum) {
-                uint64_t v = 0;
-                if ((e = cn.varint(v))) return e;
-                const int64_t value = (int64_t)v;
+                cur.push_back(OTok{at, (uint32_t)l, false, 0});
+            } else if (o == kNum || o == kDelta) {
+                int64_t value;
+                if (o == kNum) {
+                    uint64_t v = 0;
+                    if ((e = cn.varint(v))) return e;
+                    value = (int64_t)v;
+                } else {
+                    if (dpos[col] >= deltas[col].size()) return FQXV_TOK_E_DELTA_UNDERRUN;
+                    const int64_t d = unzigzag(deltas[col][dpos[col]++]);
+                    if (cur.size() >= prev.size() || !prev[cur.size()].is_num) return FQXV_TOK_E_DELTA_PRIOR;
+                    value = (int64_t)((uint64_t)prev[cur.size()].value + (uint64_t)d);
+                }
                 if (pad_pos >= npads) return FQXV_TOK_E_PAD_UNDERRUN;
-                const size_t w = natural_digits(value) + pads[pad_pos++];
-                cur.push_back(num_tok(value, w));
-            } else if (o == kDelta) {
-                if (dpos[col] >= deltas[col].size()) return FQXV_TOK_E_DELTA_UNDERRUN;
-                const int64_t d = unzigzag(deltas[col][dpos[col]++]);
-                if (cur.size() >= prev.size() || !prev[cur.size()].is_num) return FQXV_TOK_E_DELTA_PRIOR;
-                const int64_t value = (int64_t)((uint64_t)prev[cur.size()].value + (uint64_t)d);
-                if (pad_pos >= npads) return FQXV_TOK_E_PAD_UNDERRUN;
-                const size_t w = natural_digits(value) + pads[pad_pos++];
-                cur.push_back(num_tok(value, w));
+                put_num(ob, value, natural_digits(value) + pads[pad_pos++]);
+                cur.push_back(OTok{at, (uint32_t)(ob.size() - at), true, value});
             } else {
                 return FQXV_TOK_E_UNKNOWN_OP;
             }
         }
-        uint64_t nl = 0;
-        for (const auto &t : cur) {
-            out.bytes.insert(out.bytes.end(), t.bytes.begin(), t.bytes.end());
-            nl += t.bytes.size();
-        }
-        out.name_len.push_back(nl);
+        out.name_len.push_back(ob.size() - name_start);
         std::swap(prev, cur);
     }
     return FQXV_RANS_OK;

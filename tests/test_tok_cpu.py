@@ -5,7 +5,7 @@
 * The library's tokenizer host code (fqxv_b200/csrc/tok_capi.cu: role streams,
   op runs, byte planes, payload framing, error order) is compiled on its own
   with the two batch-coder calls it makes restated over the C oracle
-  (tests/c/tok_coder_stub.c), and checked against the oracle tokenizer on
+  (oracle/tok_coder_stub.c, oracle/_build/libtok_cpu.so), and checked against the oracle tokenizer on
   random blocks and on thousands of mutated payloads. The GPU coder itself is
   covered by tests/test_gpu_tok.py.
 """
@@ -22,7 +22,6 @@ import pytest
 from conftest import ROOT
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-BUILD = os.path.join(ROOT, "tests", "_build")
 CODES = {"unsupported version": 48, "truncated": 49, "varint too long": 50,
          "record count exceeds token stream": 51, "op sym underrun": 52, "op run too long": 53,
          "op columns exceed the stream bound": 54, "delta plane length mismatch": 55,
@@ -48,16 +47,8 @@ def golden_names():
 
 @pytest.fixture(scope="module")
 def tokcheck(orc):
-    os.makedirs(BUILD, exist_ok=True)
-    objs = []
-    for src, cc, flags in (("tests/c/tok_coder_stub.c", "gcc", []), ("oracle/rans_oracle.c", "gcc", ["-std=c11"]),
-                           ("oracle/rans_simd.c", "gcc", ["-std=c11"]),
-                           ("fqxv_b200/csrc/tok_capi.cu", "g++", ["-std=c++17", "-x", "c++"])):
-        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-        subprocess.check_call([cc, "-O2", "-fPIC"] + flags + ["-c", os.path.join(ROOT, src), "-o", obj])
-        objs.append(obj)
-    lib = os.path.join(BUILD, "libtokcheck.so")
-    subprocess.check_call(["g++", "-shared", "-o", lib] + objs + ["-lpthread"])
+    lib = os.path.join(ROOT, "oracle", "_build", "libtok_cpu.so")
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), lib])
     L = ctypes.CDLL(lib)
     vp, sz = ctypes.c_void_p, ctypes.c_size_t
     u64p = ctypes.POINTER(ctypes.c_uint64)
