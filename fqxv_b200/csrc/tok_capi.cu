@@ -337,9 +337,19 @@ struct OTok {
     int64_t value;
 };
 
+// The block's output bytes: written through a pointer, grown geometrically.
+struct OutBuf {
+    std::vector<uint8_t> &v;
+    size_t n = 0;
+    uint8_t *at(size_t need) {  // room for `need` more bytes at the end
+        if (n + need > v.size()) v.resize(std::max<size_t>(2 * v.size(), n + need + 4096));
+        return v.data() + n;
+    }
+};
+
 // lib.rs:684-699 num_tok: the decimal value, zero-padded on the left to
-// `width`, appended to `out`.
-void put_num(std::vector<uint8_t> &out, int64_t value, size_t width) {
+// `width`, appended; returns its length.
+size_t put_num(OutBuf &ob, int64_t value, size_t width) {
     char buf[24];
     int n = 0;
     uint64_t m = value < 0 ? 0 - (uint64_t)value : (uint64_t)value;
@@ -348,8 +358,13 @@ void put_num(std::vector<uint8_t> &out, int64_t value, size_t width) {
         m /= 10;
     } while (m);
     if (value < 0) buf[n++] = '-';
-    for (size_t k = (size_t)n; k < width; k++) out.push_back('0');
-    while (n) out.push_back((uint8_t)buf[--n]);
+    const size_t len = std::max<size_t>(width, (size_t)n);
+    uint8_t *w = ob.at(len);
+    size_t k = 0;
+    for (; k + n < len; k++) w[k] = '0';
+    while (n) w[k++] = (uint8_t)buf[--n];
+    ob.n += len;
+    return len;
 }
 
 // lib.rs:580-650: names from the decoded role streams, written straight into
@@ -358,37 +373,41 @@ int rebuild_names(uint64_t n_records, const uint8_t *counts, uint64_t ncounts, c
                   uint64_t nsl, const uint8_t *str_data, uint64_t nsd, const uint8_t *num_vals, uint64_t nnv,
                   const uint8_t *pads, uint64_t npads, const std::vector<std::vector<uint8_t>> &ops,
                   const std::vector<std::vector<uint64_t>> &deltas, BlockOut &out) {
-    std::vector<Reader> op(kCols);
+    Reader op[kCols];
     for (int c = 0; c < kCols; c++) op[c] = Reader{ops[c].data(), ops[c].size()};
-    std::vector<size_t> dpos(kCols, 0);
+    size_t dpos[kCols] = {};
     Reader cc{counts, ncounts}, cl{str_lens, nsl}, cn{num_vals, nnv};
     uint64_t str_pos = 0, pad_pos = 0;
     std::vector<OTok> prev, cur;
-    std::vector<uint8_t> &ob = out.bytes;
-    ob.reserve(nsd + 32 * n_records);
+    prev.reserve(64);
+    cur.reserve(64);
+    OutBuf ob{out.bytes};
+    out.bytes.resize(nsd + 48 * std::min<uint64_t>(n_records, 1u << 20) + 4096);
     out.name_len.reserve(n_records);
     int e;
     for (uint64_t rec = 0; rec < n_records; rec++) {
         uint64_t nt = 0;
         if ((e = cc.varint(nt))) return e;
         cur.clear();
-        const uint64_t name_start = ob.size();
+        const size_t name_start = ob.n;
         for (uint64_t t = 0; t < nt; t++) {
             const size_t col = std::min<size_t>(cur.size(), kCols - 1);
             uint8_t o = 0;
             if ((e = op[col].u8(o))) return e;
-            const uint64_t at = ob.size();
+            const size_t at = ob.n;
             if (o == kMatch) {
                 if (cur.size() >= prev.size()) return FQXV_TOK_E_MATCH;
                 const OTok p = prev[cur.size()];
-                ob.resize(at + p.len);
-                std::memcpy(ob.data() + at, ob.data() + p.off, p.len);
+                uint8_t *w = ob.at(p.len);
+                std::memcpy(w, ob.v.data() + p.off, p.len);
+                ob.n += p.len;
                 cur.push_back(OTok{at, p.len, p.is_num, p.value});
             } else if (o == kStr) {
                 uint64_t l = 0;
                 if ((e = cl.varint(l))) return e;
                 if (l > nsd || str_pos > nsd - l) return FQXV_TOK_E_STR_UNDERRUN;
-                ob.insert(ob.end(), str_data + str_pos, str_data + str_pos + l);
+                std::memcpy(ob.at(l), str_data + str_pos, l);
+                ob.n += l;
                 str_pos += l;
                 cur.push_back(OTok{at, (uint32_t)l, false, 0});
             } else if (o == kNum || o == kDelta) {
@@ -404,15 +423,16 @@ int rebuild_names(uint64_t n_records, const uint8_t *counts, uint64_t ncounts, c
                     value = (int64_t)((uint64_t)prev[cur.size()].value + (uint64_t)d);
                 }
                 if (pad_pos >= npads) return FQXV_TOK_E_PAD_UNDERRUN;
-                put_num(ob, value, natural_digits(value) + pads[pad_pos++]);
-                cur.push_back(OTok{at, (uint32_t)(ob.size() - at), true, value});
+                const size_t len = put_num(ob, value, natural_digits(value) + pads[pad_pos++]);
+                cur.push_back(OTok{at, (uint32_t)len, true, value});
             } else {
                 return FQXV_TOK_E_UNKNOWN_OP;
             }
         }
-        out.name_len.push_back(ob.size() - name_start);
+        out.name_len.push_back(ob.n - name_start);
         std::swap(prev, cur);
     }
+    out.bytes.resize(ob.n);
     return FQXV_RANS_OK;
 }
 
