@@ -386,7 +386,7 @@ def names_cpu_rate(arena, nspans, bspans, k: int):
     import ctypes
 
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
-    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "libtok_cpu.so"))
+    L = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "libcallers_cpu.so"))
     sub_b = bspans[:k]
     n_names = int(sub_b[-1, 0] + sub_b[-1, 1])
     sub_n = nspans[:n_names]

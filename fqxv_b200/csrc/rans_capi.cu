@@ -11,6 +11,7 @@
 
 #include <nvtx3/nvToolsExt.h>
 
+#include "../../include/fqxv_streams_gpu.h"
 #include "../../include/fqxv_tok_gpu.h"
 #include "frame_internal.cuh"
 #include "rans_ctx.cuh"
@@ -425,6 +426,9 @@ const char *fqxv_rans_status_message(int status) {
         case FQXV_TOK_E_DELTA_UNDERRUN: return "malformed name stream: delta underrun";
         case FQXV_TOK_E_DELTA_PRIOR: return "malformed name stream: DELTA without numeric prior";
         case FQXV_TOK_E_UNKNOWN_OP: return "malformed name stream: unknown op";
+        case FQXV_STREAM_E_CORRUPT: return "malformed lroverlap block";
+        case FQXV_PERM_E_BAD: return "malformed fqxv block: bad permutation";
+        case FQXV_PERM_E_LENGTH: return "malformed fqxv block: permutation length mismatch";
         default: return "unknown status";
     }
 }

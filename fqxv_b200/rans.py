@@ -144,6 +144,14 @@ def lib() -> ctypes.CDLL:
                                            ctypes.POINTER(ctypes.c_uint64)]
         L.fqxv_tok_decode_host.argtypes = [vp, u8p, u8p, sz, u8p, ctypes.c_uint64, u8p, ctypes.c_uint64, u8p, u8p,
                                            ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        # put_stream framing and the permutation planes (include/fqxv_streams_gpu.h)
+        L.fqxv_put_streams_host.argtypes = [vp, u8p, u8p, sz, u8p, ctypes.c_uint64, u8p,
+                                            ctypes.POINTER(ctypes.c_uint64)]
+        L.fqxv_get_streams_host.argtypes = [vp, u8p, ctypes.c_uint64, ctypes.c_uint64, sz, u8p, ctypes.c_uint64,
+                                            u8p, u8p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        L.fqxv_perm_encode_host.argtypes = [vp, u8p, ctypes.c_uint64, u8p, ctypes.c_uint64,
+                                            ctypes.POINTER(ctypes.c_uint64)]
+        L.fqxv_perm_decode_host.argtypes = [vp, u8p, ctypes.c_uint64, ctypes.c_uint64, u8p]
         L.fqxv_rans_ctx_set_profiling.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.fqxv_rans_ctx_stage_stats.argtypes = [ctypes.c_void_p, u8p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.c_int]

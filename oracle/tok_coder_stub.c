@@ -3,7 +3,7 @@
  * host code (fqxv_b200/csrc/tok_capi.cu) calls, restated over the CPU oracle
  * and run on host threads (one stream at a time per thread, as the
  * reference's callers code blocks on rayon workers). Linked with tok_capi.cu
- * into oracle/_build/libtok_cpu.so, which the tests use to check the
+ * into oracle/_build/libcallers_cpu.so, which the tests use to check the
  * tokenizer's host logic against the oracle tokenizer without a GPU and
  * bench.py times as the CPU baseline of the names workload. The product
  * library links the GPU coder instead.

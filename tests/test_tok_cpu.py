@@ -5,7 +5,7 @@
 * The library's tokenizer host code (fqxv_b200/csrc/tok_capi.cu: role streams,
   op runs, byte planes, payload framing, error order) is compiled on its own
   with the two batch-coder calls it makes restated over the C oracle
-  (oracle/tok_coder_stub.c, oracle/_build/libtok_cpu.so), and checked against the oracle tokenizer on
+  (oracle/tok_coder_stub.c, oracle/_build/libcallers_cpu.so), and checked against the oracle tokenizer on
   random blocks and on thousands of mutated payloads. The GPU coder itself is
   covered by tests/test_gpu_tok.py.
 """
@@ -47,7 +47,7 @@ def golden_names():
 
 @pytest.fixture(scope="module")
 def tokcheck(orc):
-    lib = os.path.join(ROOT, "oracle", "_build", "libtok_cpu.so")
+    lib = os.path.join(ROOT, "oracle", "_build", "libcallers_cpu.so")
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), lib])
     L = ctypes.CDLL(lib)
     vp, sz = ctypes.c_void_p, ctypes.c_size_t
