@@ -14,12 +14,14 @@ constexpr uint64_t kFrameHead = 16;                  // "FQXB" + u64 len + u32 c
 constexpr uint64_t kFrameTerm = 12;                  // "FQXB" + u64 0
 constexpr uint64_t kMaxBlockPayload = 1ull << 31;    // MAX_BLOCK_SEQ_BYTES (256 MiB) x 8
 
-// Piece kernel shape: one 1024-thread CTA per SM; a warp keeps up to
-// 2 x kCrcUnroll lines of loads in flight (2 x kCopyUnroll for the frame
-// copy, which also holds the realigned words and moves twice the bytes).
+// Piece kernel shape: one CTA per SM (the tables take 128 KiB of shared
+// memory); a warp keeps up to 2 x kCrcUnroll lines of loads in flight. The
+// frame copy also holds the realigned words and moves twice the bytes: it
+// runs 768 threads so each may keep 80 registers, 2 x kCopyUnroll lines.
 constexpr int kCrcThreads = 1024;
 constexpr int kCrcUnroll = 12;
-constexpr int kCopyUnroll = 4;
+constexpr int kCopyThreads = 768;
+constexpr int kCopyUnroll = 12;
 // Piece size 2^shift: about kCrcPieceTarget pieces per pass (four per warp
 // slot of 148 SMs x 32 warps), between 32 KiB and 256 KiB.
 constexpr int kCrcMinShift = 15;

@@ -186,15 +186,18 @@ __device__ __forceinline__ uint32_t tab_offset(uint32_t k, uint32_t b, uint32_t 
 }
 
 __device__ void build_tables(uint32_t *smem) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // entry e = 256 k + b of table k: (b << 8k) * x^(8 * 128)
-    const uint32_t e = threadIdx.x;
-    const uint32_t v = gf_mul((e & 0xFFu) << (8 * (e >> 8)), c_crc.z[128]);
+    const int lane = threadIdx.x & 31;
     uint8_t *sb = reinterpret_cast<uint8_t *>(smem);
-    for (int j = 0; j < 32; j++) {
-        const uint32_t x = __shfl_sync(0xFFFFFFFFu, v, j);
-        const uint32_t ej = (warp << 5) + j;
-        *reinterpret_cast<uint32_t *>(sb + tab_offset(ej >> 8, ej & 0xFFu, lane)) = x;
+    // entry e = 256 k + b of table k: (b << 8k) * x^(8 * 128); a warp computes
+    // 32 consecutive entries, one a lane, and writes them lane by lane
+    for (uint32_t base = threadIdx.x & ~31u; base < 1024; base += blockDim.x) {
+        const uint32_t e = base + lane;
+        const uint32_t v = gf_mul((e & 0xFFu) << (8 * (e >> 8)), c_crc.z[128]);
+        for (int j = 0; j < 32; j++) {
+            const uint32_t x = __shfl_sync(0xFFFFFFFFu, v, j);
+            const uint32_t ej = base + j;
+            *reinterpret_cast<uint32_t *>(sb + tab_offset(ej >> 8, ej & 0xFFu, lane)) = x;
+        }
     }
     for (uint32_t i = threadIdx.x; i < kZMax; i += blockDim.x) smem[kTabWords + i] = c_crc.z[i];
 }
@@ -216,8 +219,8 @@ __device__ __forceinline__ CrcPiece load_piece(const CrcPiece *p) {
 // the targets' ends); a warp prefetches its next piece's record while it
 // works on the current one, and keeps the loads of the next U lines in
 // flight while it folds in the current U.
-template <bool COPY, int U>
-__global__ void __launch_bounds__(kCrcThreads, 1)
+template <bool COPY, int U, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
     crc_piece_kernel(const uint8_t *src, uint8_t *dst, const FrameJob *job, const CrcPiece *pieces,
                      uint32_t *crc_out) {
     extern __shared__ uint32_t smem[];
@@ -834,10 +837,10 @@ static cudaError_t ensure_piece_attrs() {
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> g(mu);
     if (done[dev]) return cudaSuccess;
-    e = cudaFuncSetAttribute(crc_piece_kernel<false, kCrcUnroll>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(crc_piece_kernel<false, kCrcUnroll, kCrcThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kPieceSmem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(crc_piece_kernel<true, kCopyUnroll>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(crc_piece_kernel<true, kCopyUnroll, kCopyThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kPieceSmem);
     if (e == cudaSuccess) done[dev] = true;
     return e;
@@ -856,9 +859,9 @@ cudaError_t launch_crc_pieces(const uint8_t *src, uint8_t *dst, FrameJob *job, c
     cudaError_t e = ensure_piece_attrs();
     if (e != cudaSuccess) return e;
     if (copy)
-        crc_piece_kernel<true, kCopyUnroll><<<grid, kCrcThreads, kPieceSmem, s>>>(src, dst, job, pieces, crc_out);
+        crc_piece_kernel<true, kCopyUnroll, kCopyThreads><<<grid, kCopyThreads, kPieceSmem, s>>>(src, dst, job, pieces, crc_out);
     else
-        crc_piece_kernel<false, kCrcUnroll><<<grid, kCrcThreads, kPieceSmem, s>>>(src, dst, job, pieces, crc_out);
+        crc_piece_kernel<false, kCrcUnroll, kCrcThreads><<<grid, kCrcThreads, kPieceSmem, s>>>(src, dst, job, pieces, crc_out);
     return cudaGetLastError();
 }
 
