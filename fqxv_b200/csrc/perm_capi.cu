@@ -42,32 +42,26 @@ extern "C" {
 int fqxv_perm_encode_host(fqxv_rans_ctx *ctx, const uint32_t *order, uint64_t n, uint8_t *h_dst, uint64_t cap,
                           uint64_t *out_len) {
     if (!ctx || !h_dst || !out_len || (n && !order) || n > (1ull << 60)) return FQXV_RANS_E_INVALID_ARG;
-    cudaStream_t s;
-    uint8_t *d_planes, *d_out;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = ctx->stream;
     const uint64_t nb = 4 * n, ocap = 9 + 512 + 128 + 2 * nb;  // the smaller order fits the order-0 bound
-    {
-        std::lock_guard<std::mutex> g(ctx->mu);
-        DeviceGuard dg(ctx->device);
-        s = ctx->stream;
-        CK(ctx->io_in.ensure(std::max<uint64_t>(2 * nb, 16), s));
-        CK(ctx->io_out.ensure(std::max<uint64_t>(ocap, 16), s));
-        uint32_t *d_order = ctx->io_in.as<uint32_t>();
-        d_planes = ctx->io_in.as<uint8_t>() + nb;
-        d_out = ctx->io_out.as<uint8_t>();
-        if (n) {
-            CK(cudaMemcpyAsync(d_order, order, nb, cudaMemcpyHostToDevice, s));
-            perm_planes_kernel<<<grid_for(ctx, n / 4 + 1), 256, 0, s>>>(d_order, n, d_planes);
-            CK(cudaGetLastError());
-        }
+    CK(ctx->io_in.ensure(std::max<uint64_t>(2 * nb, 16), s));
+    CK(ctx->io_out.ensure(std::max<uint64_t>(ocap, 16), s));
+    uint32_t *d_order = ctx->io_in.as<uint32_t>();
+    uint8_t *d_planes = ctx->io_in.as<uint8_t>() + nb;
+    uint8_t *d_out = ctx->io_out.as<uint8_t>();
+    if (n) {
+        CK(cudaMemcpyAsync(d_order, order, nb, cudaMemcpyHostToDevice, s));
+        perm_planes_kernel<<<grid_for(ctx, n / 4 + 1), 256, 0, s>>>(d_order, n, d_planes);
+        CK(cudaGetLastError());
     }
     // reorder.rs:604-606: both orders, the smaller kept, ties to order-0
     fqxv_rans_span sp{0, nb}, os{0, 0};
-    int st = fqxv_rans_encode_batch(ctx, d_planes, &sp, 1, FQXV_RANS_BEST_TIE0, d_out, ocap, &os, nullptr, 1);
+    const int st = encode_batch_locked(ctx, d_planes, &sp, 1, FQXV_RANS_BEST_TIE0, d_out, ocap, &os, nullptr);
     if (st) return st;
     *out_len = os.length;
     if (os.length > cap) return FQXV_RANS_E_DST_TOO_SMALL;
-    std::lock_guard<std::mutex> g(ctx->mu);
-    DeviceGuard dg(ctx->device);
     CK(cudaMemcpyAsync(h_dst, d_out + os.offset, os.length, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return FQXV_RANS_OK;
@@ -75,30 +69,24 @@ int fqxv_perm_encode_host(fqxv_rans_ctx *ctx, const uint32_t *order, uint64_t n,
 
 int fqxv_perm_decode_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, uint64_t len, uint64_t n, uint32_t *order) {
     if (!ctx || (len && !h_src) || (n && !order) || n > (1ull << 60)) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = ctx->stream;
     const uint64_t nb = 4 * n;
-    cudaStream_t s;
-    uint8_t *d_src, *d_planes;
-    {
-        std::lock_guard<std::mutex> g(ctx->mu);
-        DeviceGuard dg(ctx->device);
-        s = ctx->stream;
-        CK(ctx->io_in.ensure(std::max<uint64_t>(len, 16), s));
-        CK(ctx->io_out.ensure(2 * nb + 16, s));  // planes, then the entries 16-byte aligned
-        d_src = ctx->io_in.as<uint8_t>();
-        d_planes = ctx->io_out.as<uint8_t>();
-        if (len) CK(cudaMemcpyAsync(d_src, h_src, len, cudaMemcpyHostToDevice, s));
-    }
+    CK(ctx->io_in.ensure(std::max<uint64_t>(len, 16), s));
+    CK(ctx->io_out.ensure(2 * nb + 16, s));  // planes, then the entries 16-byte aligned
+    uint8_t *d_src = ctx->io_in.as<uint8_t>();
+    uint8_t *d_planes = ctx->io_out.as<uint8_t>();
+    if (len) CK(cudaMemcpyAsync(d_src, h_src, len, cudaMemcpyHostToDevice, s));
     // reorder.rs:1097-1101: decode_bounded(perm_c, 4 n), then exactly 4 n bytes
     fqxv_rans_span sp{0, len}, os{0, nb};
     uint64_t got = 0;
     int32_t ds = 0;
-    const int st = fqxv_rans_decode_batch(ctx, d_src, &sp, 1, nb, d_planes, &os, &got, &ds, 1);
+    const int st = decode_batch_locked(ctx, d_src, &sp, 1, nb, d_planes, &os, &got, &ds);
     if (st != FQXV_RANS_OK && !(st >= FQXV_RANS_E_TRUNCATED && st <= FQXV_RANS_E_TRUNCATED_RENORM)) return st;
     if (ds != FQXV_RANS_OK) return FQXV_PERM_E_BAD;
     if (got != nb) return FQXV_PERM_E_LENGTH;
     if (!n) return FQXV_RANS_OK;
-    std::lock_guard<std::mutex> g(ctx->mu);
-    DeviceGuard dg(ctx->device);
     uint32_t *d_order = reinterpret_cast<uint32_t *>(d_planes + nb + ((16 - (nb & 15)) & 15));
     perm_join_kernel<<<grid_for(ctx, n), 256, 0, s>>>(d_planes, n, d_order);
     CK(cudaGetLastError());

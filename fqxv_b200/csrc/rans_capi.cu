@@ -386,6 +386,20 @@ int default_ctx(fqxv_rans_ctx **out) {
 
 }  // namespace
 
+// The batch coder for callers inside the library that already hold the
+// context's lock and device (rans_ctx.cuh).
+int fqxv::encode_batch_locked(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks, size_t nb,
+                              int mode, uint8_t *d_dst, uint64_t dst_cap, fqxv_rans_span *out_spans,
+                              int32_t *out_orders) {
+    return encode_batch_impl(ctx, d_src, blocks, nb, mode, d_dst, dst_cap, out_spans, out_orders, 1);
+}
+
+int fqxv::decode_batch_locked(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks, size_t nb,
+                              uint64_t max_len, uint8_t *d_dst, const fqxv_rans_span *out_spans,
+                              uint64_t *out_lens, int32_t *status) {
+    return decode_batch_impl(ctx, d_src, blocks, nb, max_len, d_dst, out_spans, out_lens, status, 1);
+}
+
 extern "C" {
 
 const char *fqxv_rans_status_message(int status) {

@@ -163,6 +163,16 @@ void *mapped_device_ptr(const void *h);
 
 }  // namespace fqxv
 
+namespace fqxv {
+// fqxv_rans_encode_batch / fqxv_rans_decode_batch (persistent form) for
+// callers that already hold ctx->mu and have the context's device current.
+int encode_batch_locked(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks, size_t nb, int mode,
+                        uint8_t *d_dst, uint64_t dst_cap, fqxv_rans_span *out_spans, int32_t *out_orders);
+int decode_batch_locked(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks, size_t nb,
+                        uint64_t max_len, uint8_t *d_dst, const fqxv_rans_span *out_spans, uint64_t *out_lens,
+                        int32_t *status);
+}  // namespace fqxv
+
 struct fqxv_rans_ctx {
     int device = 0;
     int sms = 148;
