@@ -40,14 +40,6 @@ void put_varint(std::vector<uint8_t> &out, uint64_t v) {  // fqxv-bytes lib.rs:1
 uint64_t zigzag(int64_t d) { return ((uint64_t)d << 1) ^ (uint64_t)(d >> 63); }
 int64_t unzigzag(uint64_t z) { return (int64_t)((z >> 1) ^ (0 - (z & 1))); }
 
-// lib.rs:256-265
-size_t natural_digits(int64_t v) {
-    if (v <= 0) return 1;
-    size_t d = 0;
-    for (uint64_t x = (uint64_t)v; x; x /= 10) d++;
-    return d;
-}
-
 template <class F>
 void parallel_for(size_t n, F &&f) {
     size_t nt = std::min<size_t>(n, std::max(1u, std::min(32u, std::thread::hardware_concurrency())));
@@ -115,7 +107,11 @@ void build_roles(const uint8_t *names, const fqxv_rans_span *spans, uint64_t fir
             if (p && p->len == t.len && std::memcmp(p->p, t.p, t.len) == 0) {
                 ops[col].push_back(kMatch);
             } else if (t.is_num) {
-                const uint8_t pad = (uint8_t)(t.len - natural_digits(t.value));
+                // t.len - natural_digits(t.value): the leading zeros, all but a
+                // last lone digit
+                uint32_t lz = 0;
+                while (lz + 1 < t.len && t.p[lz] == '0') lz++;
+                const uint8_t pad = (uint8_t)lz;
                 if (p && p->is_num) {
                     ops[col].push_back(kDelta);
                     deltas[col].push_back(zigzag((int64_t)((uint64_t)t.value - (uint64_t)p->value)));
@@ -347,9 +343,11 @@ struct OutBuf {
     }
 };
 
-// lib.rs:684-699 num_tok: the decimal value, zero-padded on the left to
-// `width`, appended; returns its length.
-size_t put_num(OutBuf &ob, int64_t value, size_t width) {
+// lib.rs:684-699 num_tok with the width lib.rs:620-634 gives it: the decimal
+// value, zero-padded on the left to natural_digits(value) + pad, appended;
+// returns its length. The digits are generated once and give the natural
+// width too.
+size_t put_num(OutBuf &ob, int64_t value, size_t pad) {
     char buf[24];
     int n = 0;
     uint64_t m = value < 0 ? 0 - (uint64_t)value : (uint64_t)value;
@@ -357,8 +355,9 @@ size_t put_num(OutBuf &ob, int64_t value, size_t width) {
         buf[n++] = (char)('0' + m % 10);
         m /= 10;
     } while (m);
+    const size_t natural = value > 0 ? (size_t)n : 1;  // lib.rs:256-265
     if (value < 0) buf[n++] = '-';
-    const size_t len = std::max<size_t>(width, (size_t)n);
+    const size_t len = std::max<size_t>(natural + pad, (size_t)n);
     uint8_t *w = ob.at(len);
     size_t k = 0;
     for (; k + n < len; k++) w[k] = '0';
@@ -423,7 +422,7 @@ int rebuild_names(uint64_t n_records, const uint8_t *counts, uint64_t ncounts, c
                     value = (int64_t)((uint64_t)prev[cur.size()].value + (uint64_t)d);
                 }
                 if (pad_pos >= npads) return FQXV_TOK_E_PAD_UNDERRUN;
-                const size_t len = put_num(ob, value, natural_digits(value) + pads[pad_pos++]);
+                const size_t len = put_num(ob, value, pads[pad_pos++]);
                 cur.push_back(OTok{at, (uint32_t)len, true, value});
             } else {
                 return FQXV_TOK_E_UNKNOWN_OP;
