@@ -100,3 +100,36 @@ def _build_c_caller(tmp_path):
 
 def test_plain_c_caller_compiles_and_links(tmp_path):
     assert os.path.exists(_build_c_caller(tmp_path))
+
+
+def test_frame_tok_stream_entry_points_validate_arguments():
+    """The added C-ABI calls reject bad arguments before touching a device,
+    and their host-only arithmetic needs none."""
+    from fqxv_b200 import rans
+
+    L = rans.lib()
+    null = ctypes.c_void_p()
+    n = ctypes.c_uint64(0)
+    assert L.fqxv_crc32c_batch(null, null, null, 0, null) == 16
+    assert L.fqxv_frame_blocks(null, null, null, 0, 0, null, 0, null, null, ctypes.byref(n)) == 16
+    sz = ctypes.c_size_t(0)
+    t = ctypes.c_int(0)
+    assert L.fqxv_read_blocks(null, null, 0, 0, null, null, null, ctypes.byref(sz), ctypes.byref(n),
+                              ctypes.byref(t)) == 16
+    assert L.fqxv_tok_encode_host(null, null, null, 0, null, 0, null, 0, null, None) == 16
+    assert L.fqxv_tok_decode_host(null, null, null, 0, null, 0, null, 0, null, null, None, None) == 16
+    assert L.fqxv_put_streams_host(null, null, null, 0, null, 0, null, None) == 16
+    assert L.fqxv_perm_decode_host(null, null, 0, 0, null) == 16
+    spans = (ctypes.c_uint64 * 4)(0, 10, 10, 5)
+    assert L.fqxv_frame_blocks_bound(spans, 2, 0) == 16 * 2 + 15
+    assert L.fqxv_frame_blocks_bound(spans, 2, 1) == 16 * 2 + 15 + 12
+
+
+def test_added_status_messages():
+    from fqxv_b200 import rans
+
+    assert rans.status_message(33) == "corrupted fqxv data: block (crc mismatch)"
+    assert rans.status_message(48) == "malformed name stream: unsupported version"
+    assert rans.status_message(61) == "malformed name stream: unknown op"
+    assert rans.status_message(64) == "malformed lroverlap block"
+    assert rans.status_message(66) == "malformed fqxv block: permutation length mismatch"
