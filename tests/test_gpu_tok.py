@@ -8,7 +8,7 @@ import random
 import numpy as np
 import pytest
 
-from test_tok_cpu import CODES, _oracle_decode, mutate, random_blocks  # noqa: F401
+from test_tok_cpu import CODES, _oracle_decode, edge_blocks, mutate, random_blocks  # noqa: F401
 
 pytestmark = pytest.mark.gpu
 
@@ -90,3 +90,13 @@ def test_large_batch_round_trip(tok, T):
     for k in (0, 77, 199):
         assert payloads[k] == T.encode(blocks[k])
     assert tok.decode_blocks(payloads) == blocks
+
+
+def test_edge_cases_match_oracle(tok, T, orc):
+    blocks = edge_blocks()
+    want = [T.encode(b) for b in blocks]
+    assert tok.encode_blocks(blocks) == want
+    got, st = tok.decode_blocks(want, raise_on_error=False)
+    for g, s, w in zip(got, st, want):
+        assert (int(s), g) == _oracle_decode(T, orc, w)
+    assert int(st[4]) == CODES["op run too long"]

@@ -139,3 +139,16 @@ def test_host_framing_matches_oracle(SO, orc, callers, golden):
         k_ok = len(ogot) if ost else len(raws)
         assert got[:k_ok] == ogot[:k_ok] and all(s == 0 for s in st[:k_ok])
         assert all(s == 64 for s in st[k_ok:])
+
+
+def test_host_framing_edges(SO, callers):
+    # no frames; a buffer that ends exactly after the last frame; a zero-length
+    # frame; a truncated length varint
+    assert lib_get(callers, b"abc", 3, 0) == (0, [], [])
+    frames = lib_put(callers, [b"", b"q" * 40])
+    buf = b"".join(frames)
+    assert lib_get(callers, buf, 0, 2) == (0, [b"", b"q" * 40], [0, 0])
+    r, got, st = lib_get(callers, buf, 0, 3)
+    assert r == 64 and st == [0, 0, 64]
+    r, got, st = lib_get(callers, b"\x80", 0, 1)
+    assert r == 64 and st == [64]

@@ -199,3 +199,26 @@ def test_host_code_error_order_matches_oracle(tokcheck, tok_oracle, orc, golden_
         assert (st, names) == _oracle_decode(T, orc, p)
         statuses.add(st)
     assert len(statuses) >= 6
+
+
+def edge_blocks():
+    return [
+        [b"", b"", b"a"],                                          # empty names
+        [b"000", b"0", b"00", b"0000000000000000007", b"7"],       # zero padding, value 0
+        [b"1234567890123456789", b"1234567890123456788"],          # 19 digits: a string token
+        [b"x" + b"1" * 18, b"x" + b"1" * 17 + b"2"],               # 18 digits: numeric, delta
+        [b":".join(b"%d" % k for k in range(80)), b":".join(b"%d" % (k + 1) for k in range(80))],  # > 64 tokens
+        [b"A:1", b"A:1", b"A:1:2", b"A", b"A:3"],                  # token counts change between names
+    ]
+
+
+def test_host_code_edge_cases_match_oracle(tokcheck, tok_oracle, orc):
+    T = tok_oracle
+    blocks = edge_blocks()
+    want = [T.encode(b) for b in blocks]
+    assert _encode(tokcheck, blocks) == want
+    for (st, names), w in zip(_decode(tokcheck, want), want):
+        assert (st, names) == _oracle_decode(T, orc, w)
+    # names of more than 64 tokens share the last column, which the
+    # reference's decode rejects ("op run too long"); so does this one
+    assert _decode(tokcheck, [want[4]])[0][0] == CODES["op run too long"]
