@@ -12,9 +12,10 @@ seeded copy of the workload; blocks are independent, there is no collective
 on the data path). L2 is flushed (a 256 MiB write) before every timed step.
 
 Workloads (seeded synthetic data of the benchmark shapes):
-  config1  64 x 1 MiB full-range quality, order-1                 (default)
-  config0  1 x 1 MiB binned quality, order-0
   config2  4096 mixed blocks 4 KiB - 4 MiB, both orders, keep the smaller
+           (tokenizer tie rule)                                    (default)
+  config0  1 x 1 MiB binned quality, order-0
+  config1  64 x 1 MiB full-range quality, order-1
   config3  config2 (CPU-encoded) + ONT long-read blocks, decode only
   batch0 / batch1 / batch1f   2048 x 512 KiB binned order-0 / binned order-1 /
            full-range order-1: peak batched throughput of one order
@@ -25,6 +26,13 @@ Workloads (seeded synthetic data of the benchmark shapes):
   crc      CRC-32C of 4096 payloads 4 KiB - 4 MiB (crates/fqxv/src/crc.rs)
   frame    block frames of the same payloads: write (copy + CRC-32C, terminator)
            then read back with every CRC verified (container/block.rs)
+
+Besides the timed round trip, a run of an encoding workload checks every
+stream the GPU wrote against the CPU restatement of the reference encoder
+(`byte_identical_blocks`) and decodes the CPU's streams on the GPU; times the
+plain one-block-per-launch form of the same batch (`plain_per_block`); and,
+on one GPU, runs a short serving pass (`serving`: Poisson arrivals at two
+offered loads, p50/p99 latency against plain per-request calls).
 
 The reference arm (`--impl reference`) times the reference's CPU coder -- the
 C restatement of fqxv-rans (AVX-512/AVX2 order-0, scalar order-1) -- with all
@@ -727,16 +735,15 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args, rank: int) -> None:
-    """config4: requests arrive as a Poisson process at offered loads (fractions
-    of the measured batched capacity); 70% decompress / 30% compress; sizes
-    log-uniform 16 KiB - 64 MiB; stream types of configs 2 and 3. The server
-    admits by device memory under a 40 GB cap and batches continuously; the
-    same schedule is also run through plain per-request calls."""
-    if rank != 0:
-        return
+def serving_levels(seed: int, nreq: int, loads, workers: int) -> dict:
+    """config4's serving loop: requests arrive as a Poisson process at offered
+    loads (fractions of the measured batched capacity); 70% decompress / 30%
+    compress; sizes log-uniform 16 KiB - 64 MiB; stream types of configs 2
+    and 3. The server admits by device memory under a 40 GB cap and batches
+    continuously; the same schedule also runs through plain per-request
+    calls. Returns the capacity and, per load, p50/p99 of both forms and
+    whether every result is byte-identical to the expected stream."""
     import queue as _queue
-    import random
 
     import torch
 
@@ -744,36 +751,35 @@ def run_serving(args, rank: int) -> None:
     from fqxv_b200.serve import Server
     from oracle import oracle
 
-    rng = np.random.default_rng(args.seed)
+    rng = np.random.default_rng(seed)
     kinds = ["binned", "full", "acgt", "names", "ont"]
-    nreq = args.requests
     reqs = []
     for i in range(nreq):
         size = int(np.exp(rng.uniform(np.log(16 << 10), np.log(64 << 20))))
         kind = kinds[int(rng.integers(0, len(kinds)))]
         if kind == "ont":
-            data = W.ont_reads(max(1, size // 8000 + 1), args.seed + i)[:size]
+            data = W.ont_reads(max(1, size // 8000 + 1), seed + i)[:size]
         else:
-            data = W.GENERATORS[kind](size, args.seed + i)
+            data = W.GENERATORS[kind](size, seed + i)
         raw = data.tobytes()
+        e0, e1 = oracle.encode(raw, 0), oracle.encode(raw, 1)
+        best = e1 if len(e1) < len(e0) else e0
         if rng.random() < 0.7:
-            e0, e1 = oracle.encode(raw, 0), oracle.encode(raw, 1)
-            reqs.append(("dec", e1 if len(e1) < len(e0) else e0, len(raw)))
+            reqs.append(("dec", best, len(raw), raw))
         else:
-            reqs.append(("enc", raw, len(raw)))
+            reqs.append(("enc", raw, len(raw), best))
     total = sum(r[2] for r in reqs)
     torch.cuda.init()
-    expect = [None] * nreq
 
     # One long-lived server (created and warmed once, as in deployment).
-    srv = Server(device=0, workers=args.workers, hbm_cap=40 << 30)
+    srv = Server(device=0, workers=workers, hbm_cap=40 << 30)
 
     def run_server(arrivals):
         lat = [0.0] * nreq
         b0 = srv.stats()["batches"]
         ids = [None] * nreq
         t0 = time.perf_counter()
-        for i, (k, d, n) in enumerate(reqs):
+        for i, (k, d, n, _) in enumerate(reqs):
             wait = arrivals[i] - (time.perf_counter() - t0)
             if wait > 0:
                 time.sleep(wait)
@@ -800,7 +806,7 @@ def run_serving(args, rank: int) -> None:
                 if item is None:
                     return
                 i, t_arr = item
-                k, d, n = reqs[i]
+                k, d, n, _ = reqs[i]
                 outs[i] = rans.decode(d) if k == "dec" else rans.encode(d, rans.Order.BestTie0)
                 done[i] = time.perf_counter()
         th = threading.Thread(target=worker)
@@ -820,16 +826,18 @@ def run_serving(args, rank: int) -> None:
             lat[i] = (done[i] - arr_abs[i]) * 1e3
         return outs, lat, wall
 
+    # expected result of each request: the original bytes (decompress) or
+    # the reference encoder's best-order stream (compress)
+    expect = [r[3] for r in reqs]
     # warm-up pass, then capacity: everything submitted at once
     run_server([0.0] * nreq)
     outs, lat, wall, st = run_server([0.0] * nreq)
-    for i, (k, d, n) in enumerate(reqs):
-        expect[i] = outs[i]
+    cap_ok = all(o == e for o, e in zip(outs, expect))
     cap_gbs = total / wall / 1e9
     levels = []
-    for load in args.loads:
+    for load in loads:
         lam = load * cap_gbs * 1e9 / (total / nreq)  # requests per second
-        arrivals = list(np.cumsum(np.random.default_rng(args.seed + int(load * 100)).exponential(1.0 / lam, nreq)))
+        arrivals = list(np.cumsum(np.random.default_rng(seed + int(load * 100)).exponential(1.0 / lam, nreq)))
         outs, lat, wall, st = run_server(arrivals)
         same = all(o == e for o, e in zip(outs, expect))
         outs_p, lat_p, wall_p = run_plain(arrivals)
@@ -845,16 +853,95 @@ def run_serving(args, rank: int) -> None:
                                   "byte_identical": bool(same_p)},
         })
     srv.close()
+    return {"requests": nreq, "bytes": total, "capacity_gbs": round(cap_gbs, 3), "capacity_byte_identical": cap_ok,
+            "levels": levels}
+
+
+def run_serving(args, rank: int) -> None:
+    """config4 on its own line: every offered load of --loads."""
+    if rank != 0:
+        return
+    res = serving_levels(args.seed, args.requests, args.loads, args.workers)
+    levels = res["levels"]
     line = {
         "metric": "rANS Nx16 serving: p50/p99 latency vs offered load (GB/s of uncompressed bytes)",
         "value": levels[-1]["served"]["gbs"], "unit": "GB/s", "n_gpus": 1, "steps": len(args.loads),
         "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "config4", "requests": nreq, "bytes": total, "decompress_fraction": 0.7,
-                   "sizes": "log-uniform 16 KiB - 64 MiB", "hbm_cap_bytes": 40 << 30, "workers": args.workers},
-        "capacity_gbs": round(cap_gbs, 3), "levels": levels,
+        "config": {"workload": "config4", "requests": res["requests"], "bytes": res["bytes"],
+                   "decompress_fraction": 0.7, "sizes": "log-uniform 16 KiB - 64 MiB", "hbm_cap_bytes": 40 << 30,
+                   "workers": args.workers},
+        "capacity_gbs": res["capacity_gbs"], "levels": levels,
     }
     print(json.dumps(line), flush=True)
+
+
+def check_identity(codec, data, spans, order, d_enc, enc_spans, decode_only) -> dict:
+    """Every stream the GPU wrote against the CPU restatement of the
+    reference encoder (same order mode, same tie rule), block by block; and
+    the CPU's streams decoded on the GPU against the input. Decode-only
+    workloads check the GPU decode of the CPU's streams only."""
+    import torch
+
+    from oracle import oracle
+
+    nthreads = os.cpu_count() or 1
+    n_bytes = int(spans[:, 1].sum())
+    out = {}
+    if not decode_only:
+        ref, roff, rlen = oracle.encode_batch(data, spans[:, 0], spans[:, 1], order, nthreads)
+        total = int(enc_spans[-1, 0] + enc_spans[-1, 1])
+        got = d_enc[:total].cpu().numpy()
+        same = 0
+        for i in range(len(spans)):
+            o, ln = int(enc_spans[i, 0]), int(enc_spans[i, 1])
+            if ln == int(rlen[i]) and np.array_equal(got[o:o + ln], ref[int(roff[i]):int(roff[i] + rlen[i])]):
+                same += 1
+        out["blocks"] = "%d/%d" % (same, len(spans))
+        out["encoder"] = "oracle.encode_batch mode %d (C restatement of fqxv-rans scalar.rs/model.rs)" % order
+        arena, cspans = ref, np.stack([roff, rlen], 1)
+    else:
+        arena, cspans = cpu_encoded(data, spans, 0)
+    d_ref = torch.from_numpy(np.ascontiguousarray(arena)).to("cuda")
+    d_dec, lens, st = codec.decode_batch(d_ref, cspans, spans)
+    torch.cuda.synchronize()
+    ok = bool((st == 0).all()) and np.array_equal(d_dec[:n_bytes].cpu().numpy(), data[:n_bytes])
+    out["cpu_streams_gpu_decoded"] = ok
+    if decode_only:
+        out["blocks"] = "%d/%d" % (int((st == 0).sum()) if ok else 0, len(spans))
+    assert ok, "GPU decode of the CPU encoder's streams differs from the input"
+    del d_ref, d_dec
+    return out
+
+
+def stage_roofline(stages: dict, steps: int, workload: str) -> dict:
+    """The dominant stage against the HBM roofline. A stage can be several
+    launches that run side by side on separate CUDA streams (the decode
+    groups), so its time is its wall time on the device per step (first
+    launch start to last launch end), and its algorithmic bytes are those of
+    all its launches in the step: decode moves compressed + n bytes of the
+    streams it decodes, encode n + the words written, pack the words read +
+    the stream written; tables are on chip and excluded."""
+    pk = peaks()
+    timed = {k: v for k, v in stages.items() if v["launches"] > 0}
+    dom = max(timed, key=lambda k: timed[k]["wall_ms"])
+    wall_ms = timed[dom]["wall_ms"] / steps
+    alg_bytes = timed[dom]["bytes"] / steps
+    achieved = alg_bytes / (wall_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tr = json.load(f)
+        ent = tr.get(workload, {}).get(dom)
+        if ent:
+            traffic = ent.get("dram_bytes_per_step")
+    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 6), "traffic": traffic,
+            "alg_bytes_per_step": int(alg_bytes), "wall_ms_per_step": round(wall_ms, 4),
+            "launches_per_step": timed[dom]["launches"] / steps,
+            "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"
+            if pk["source"] == "measured" else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"}
 
 
 def main() -> None:
@@ -863,7 +950,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="config1",
+    ap.add_argument("--workload", default="config2",
                     choices=["config1", "config0", "config2", "config3", "config4", "batch0", "batch1", "batch1f",
                              "cpu_single", "crc", "frame", "names"])
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
@@ -874,6 +961,10 @@ def main() -> None:
                     help="configs 1/2 and batch*: number of blocks (0 = the benchmark shape; smaller for profiler captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-identity", action="store_true",
+                    help="skip the check of every GPU stream against the CPU encoder")
+    ap.add_argument("--serving-requests", type=int, default=24,
+                    help="requests of the serving pass in the default line (0: no serving pass)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -943,6 +1034,11 @@ def main() -> None:
     torch.cuda.synchronize()
     assert (st == 0).all() and torch.equal(d_dec[:n_bytes], d_src[:n_bytes]), "round trip mismatch"
 
+    # ---- byte identity against the CPU encoder (outside the timed region) -----
+    identity = None
+    if not args.no_identity and rank == 0:
+        identity = check_identity(codec, data, spans, order, d_enc, enc_spans, decode_only)
+
     # ---- timed region ---------------------------------------------------
     codec.stage_stats(reset=True)
     codec.set_profiling(True)
@@ -983,30 +1079,7 @@ def main() -> None:
     value = world * n_bytes * args.steps / (total_ms * 1e-3) / 1e9
 
     # ---- the dominant kernel against the HBM roofline -------------------------
-    pk = peaks()
-    timed = {k: v for k, v in stages.items() if v["launches"] > 0}
-    dom = max(timed, key=lambda k: timed[k]["ms"])
-    launches = timed[dom]["launches"]
-    per_launch_ms = timed[dom]["ms"] / launches
-    # Algorithmic bytes of a launch: the stage reads its input once and writes
-    # its output once (decode: compressed + n of the streams it decodes;
-    # encode: n + the words written); tables are on chip and excluded. The
-    # library accumulates them per stage, so a stage split over several
-    # launches (decode groups) divides them by its launch count.
-    alg_bytes = timed[dom]["bytes"] / launches
-    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            tr = json.load(f)
-        ent = tr.get(args.workload, {}).get(dom)
-        if ent:
-            traffic = ent.get("dram_bytes_per_launch")
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": pk["hbm_gbs"],
-                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 5), "traffic": traffic,
-                "alg_bytes_per_launch": int(alg_bytes), "launch_ms": round(per_launch_ms, 4),
-                "peak_source": pk["source"] + " (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"}
+    roofline = stage_roofline(stages, args.steps, args.workload)
     gpu_launches = int(sum(v["launches"] for v in stages.values()))
 
     # ---- plain one-block-per-launch form (same bytes) -------------------------
@@ -1020,7 +1093,10 @@ def main() -> None:
         b.record(cs)
         b.synchronize()
         ok = bool((st == 0).all()) and torch.equal(d_dec[:n_bytes], d_src[:n_bytes])
-        plain = {"gbs": round(n_bytes / (a.elapsed_time(b) * 1e-3) / 1e9, 4), "round_trip_ok": ok}
+        pg = n_bytes / (a.elapsed_time(b) * 1e-3) / 1e9
+        own = n_bytes * args.steps / (total_ms * 1e-3) / 1e9
+        plain = {"gbs": round(pg, 4), "round_trip_ok": ok, "batched_over_plain": round(own / pg, 2),
+                 "form": "one launch per block and stage, same kernels, same bytes"}
 
     # ---- end to end through the C ABI with pinned host buffers ---------------
     h_src = torch.from_numpy(data).pin_memory().numpy()
@@ -1097,16 +1173,23 @@ def main() -> None:
             "encode_gbs": None if decode_only else round(world * n_bytes * args.steps / (enc_ms * 1e-3) / 1e9, 4),
             "decode_gbs": round(world * n_bytes * args.steps / (dec_ms * 1e-3) / 1e9, 4),
             "plain_per_block": plain,
+            "byte_identical_blocks": identity["blocks"] if identity else None,
+            "identity": identity,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": gpu_launches,
-            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "bytes": v["bytes"]}
-                       for k, v in stages.items()},
+            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "wall_ms": round(v["wall_ms"], 4),
+                           "bytes": v["bytes"]}
+                       for k, v in stages.items() if v["launches"]},
             "clocks": clocks,
         }
-        print(json.dumps(line), flush=True)
     codec.close()
+    if rank == 0 and world == 1 and args.serving_requests > 0 and args.workload == "config2":
+        # a short serving pass (config4's loop) after the batch measurements
+        line["serving"] = serving_levels(args.seed, args.serving_requests, [0.5, 1.0], args.workers)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -17,7 +17,7 @@ from . import rans
 
 class StageStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double),
-                ("bytes", ctypes.c_uint64)]
+                ("bytes", ctypes.c_uint64), ("wall_ms", ctypes.c_double)]
 
 
 # format.rs:252-266 StreamLoc, as include/fqxv_frame_gpu.h lays it out.
@@ -84,7 +84,9 @@ class Codec:
     def decode_batch(self, d_src, spans, out_spans, max_len: int | None = None, d_dst=None,
                      persistent: bool = True, raise_on_error: bool = True):
         """Decode streams `spans` of d_src into d_dst at out_spans (offset,
-        capacity). Returns (d_dst, out_lens, status)."""
+        capacity). Returns (d_dst, out_lens, status). With raise_on_error
+        False, per-stream statuses (malformed streams, and device waits that
+        timed out) come back in `status` instead of raising."""
         import torch
 
         s = _spans(spans)
@@ -99,7 +101,7 @@ class Codec:
         st = self._lib.fqxv_rans_decode_batch(self._h, d_src.data_ptr(), s.ctypes.data, nb, ml,
                                               d_dst.data_ptr(), o.ctypes.data, lens.ctypes.data,
                                               status.ctypes.data, 1 if persistent else 0)
-        if st and (raise_on_error or st not in rans.MALFORMED):
+        if st and (raise_on_error or st not in rans.STREAM_STATUSES):
             rans.raise_for(st)
         return d_dst, lens, status
 
@@ -232,4 +234,12 @@ class Codec:
         rans.raise_for(self._lib.fqxv_rans_ctx_stage_stats(self._h, ctypes.cast(arr, ctypes.c_void_p), 16,
                                                            ctypes.byref(n), 1 if reset else 0))
         return {arr[i].name.decode(): {"launches": int(arr[i].launches), "ms": float(arr[i].ms),
-                                       "bytes": int(arr[i].bytes)} for i in range(n.value)}
+                                       "bytes": int(arr[i].bytes), "wall_ms": float(arr[i].wall_ms)}
+                for i in range(n.value)}
+
+    def _test_set_wait_polls(self, polls: int) -> None:
+        """Test-only (include/fqxv_rans_gpu_testing.h): polls of a decode
+        kernel's first wait for its table copy; 0 makes every staged stream
+        report FQXV_RANS_E_TIMEOUT."""
+        self._lib.fqxv_rans_ctx_test_set_wait_polls.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        rans.raise_for(self._lib.fqxv_rans_ctx_test_set_wait_polls(self._h, int(polls)))

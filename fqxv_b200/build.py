@@ -32,10 +32,8 @@ def nvcc() -> str:
 
 def _inputs() -> list[str]:
     files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    files.append(os.path.join(ROOT, "include", "fqxv_rans_gpu.h"))
-    files.append(os.path.join(ROOT, "include", "fqxv_frame_gpu.h"))
-    files.append(os.path.join(ROOT, "include", "fqxv_tok_gpu.h"))
-    files.append(os.path.join(ROOT, "include", "fqxv_streams_gpu.h"))
+    inc = os.path.join(ROOT, "include")
+    files += [os.path.join(inc, f) for f in sorted(os.listdir(inc)) if f.endswith(".h")]
     files.append(os.path.abspath(__file__))
     return files
 

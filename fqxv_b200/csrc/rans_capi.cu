@@ -12,6 +12,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include "../../include/fqxv_streams_gpu.h"
+#include "../../include/fqxv_rans_gpu_testing.h"
 #include "../../include/fqxv_tok_gpu.h"
 #include "frame_internal.cuh"
 #include "rans_ctx.cuh"
@@ -334,14 +335,15 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             if (persistent) {
                 const int grid = (int)std::min<size_t>(m, (size_t)ctx->sms * per_sm);
                 cudaEvent_t t0 = ctx->timer.begin(as);
-                launch_dec_run(cls, d_src, dS, dl + base[g], (int)m, dT, d_dst, queue + 4 * g, grid, smem[g], as);
+                launch_dec_run(cls, d_src, dS, dl + base[g], (int)m, dT, d_dst, queue + 4 * g, grid, smem[g],
+                               ctx->first_polls, as);
                 ctx->timer.end(stage, t0, as);
             } else {
                 for (size_t j = 0; j < m; j++) {
                     CK(cudaMemsetAsync(queue + 4 * g, 0, 4, as));
                     cudaEvent_t t0 = ctx->timer.begin(as);
                     launch_dec_run(cls, d_src, dS, dl + base[g] + j, 1, dT, d_dst, queue + 4 * g, 1,
-                                   dec_smem_bytes(cls, ps[lists[g][j]].nd), as);
+                                   dec_smem_bytes(cls, ps[lists[g][j]].nd), ctx->first_polls, as);
                     ctx->timer.end(stage, t0, as);
                 }
             }
@@ -615,6 +617,14 @@ int fqxv_rans_ctx_set_profiling(fqxv_rans_ctx *ctx, int on) {
     return FQXV_RANS_OK;
 }
 
+int fqxv_rans_ctx_test_set_wait_polls(fqxv_rans_ctx *ctx, uint32_t polls) {
+    if (!ctx) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->first_polls = polls;
+    for (auto *c : ctx->sub) c->first_polls = ctx->first_polls;
+    return FQXV_RANS_OK;
+}
+
 int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int cap, int *n, int reset) {
     if (!ctx || !n || (cap > 0 && !out)) return FQXV_RANS_E_INVALID_ARG;
     std::lock_guard<std::mutex> g(ctx->mu);
@@ -625,12 +635,14 @@ int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int
         out[k].launches = ctx->timer.launches[i];
         out[k].ms = ctx->timer.ms[i];
         out[k].bytes = ctx->timer.bytes[i];
+        out[k].wall_ms = ctx->timer.wall_ms[i];
     }
     *n = k;
     if (reset) {
         for (int i = 0; i < kStages; i++) {
             ctx->timer.launches[i] = 0;
             ctx->timer.ms[i] = 0.0;
+            ctx->timer.wall_ms[i] = 0.0;
             ctx->timer.bytes[i] = 0;
         }
     }
@@ -705,6 +717,7 @@ int ensure_subs(fqxv_rans_ctx *ctx, size_t k) {
         fqxv_rans_ctx *c = nullptr;
         const int st = fqxv_rans_ctx_create(ctx->device, &c);
         if (st != FQXV_RANS_OK) return st;
+        c->first_polls = ctx->first_polls;
         ctx->sub.push_back(c);
     }
     return FQXV_RANS_OK;

@@ -83,7 +83,13 @@ const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_sc
                                           "frame_walk"};
 
 // CUDA-event brackets around each kernel launch on the context's stream.
-// Durations are collected after the call's final synchronisation.
+// Durations are collected after the call's final synchronisation. Launches of
+// one stage can run side by side on several streams (the decode groups), so
+// besides the sum of launch durations (`ms`) the timer keeps each stage's
+// wall time on the device (`wall_ms`): from its first launch's start to its
+// last launch's end within a call, measured against an event recorded on the
+// context's stream before the call's first launch (every later launch, on any
+// of the context's streams, is ordered after it).
 struct StageTimer {
     bool on = false;
     struct Pending {
@@ -92,7 +98,9 @@ struct StageTimer {
     };
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> pool;
+    cudaEvent_t origin = nullptr;
     double ms[kStages] = {};
+    double wall_ms[kStages] = {};
     uint64_t launches[kStages] = {};
     uint64_t bytes[kStages] = {};   // algorithmic bytes moved by the stage's launches
     cudaEvent_t get() {
@@ -108,9 +116,14 @@ struct StageTimer {
         }
         return e;
     }
-    // Returns the start event (or null); pass it to end().
+    // Returns the start event (or null); pass it to end(). The first launch
+    // of a call also records the call's origin on the same stream.
     cudaEvent_t begin(cudaStream_t s) {
         if (!on) return nullptr;
+        if (!origin) {
+            origin = get();
+            if (origin) cudaEventRecord(origin, s);
+        }
         cudaEvent_t a = get();
         if (a) cudaEventRecord(a, s);
         return a;
@@ -124,14 +137,31 @@ struct StageTimer {
         pending.push_back({stage, a, b});
     }
     void collect() {
+        double lo[kStages], hi[kStages];
+        for (int i = 0; i < kStages; i++) {
+            lo[i] = 1e300;
+            hi[i] = -1e300;
+        }
         for (auto &p : pending) {
             float t = 0.f;
             if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.stage] += t;
             else cudaGetLastError();
+            float ta = 0.f, tb = 0.f;
+            if (origin && cudaEventElapsedTime(&ta, origin, p.a) == cudaSuccess &&
+                cudaEventElapsedTime(&tb, origin, p.b) == cudaSuccess) {
+                lo[p.stage] = std::min(lo[p.stage], (double)ta);
+                hi[p.stage] = std::max(hi[p.stage], (double)tb);
+            } else {
+                cudaGetLastError();
+            }
             pool.push_back(p.a);
             pool.push_back(p.b);
         }
+        for (int i = 0; i < kStages; i++)
+            if (hi[i] >= lo[i]) wall_ms[i] += hi[i] - lo[i];
         pending.clear();
+        if (origin) pool.push_back(origin);
+        origin = nullptr;
     }
     void release() {
         for (auto &p : pending) {
@@ -139,6 +169,8 @@ struct StageTimer {
             pool.push_back(p.b);
         }
         pending.clear();
+        if (origin) pool.push_back(origin);
+        origin = nullptr;
         for (auto e : pool) cudaEventDestroy(e);
         pool.clear();
     }
@@ -191,6 +223,10 @@ struct fqxv_rans_ctx {
     fqxv::HostBuf h_stage;
     fqxv::HostBuf h_io;
     fqxv::StageTimer timer;
+    // Polls of a decode kernel's first wait for its table copy (a drain with
+    // the full bound follows a wait that gives up). Only the test-only
+    // setter in fqxv_rans_gpu_testing.h lowers it.
+    uint32_t first_polls = fqxv::kWaitPolls;
     // host-buffer batches cut into chunks run one chunk per sub-context
     std::vector<fqxv_rans_ctx *> sub;
     template <class F>

@@ -345,20 +345,37 @@ struct TableStager {
                 : "memory");
         }
     }
-    __device__ bool wait() {
+    // Polls the barrier's current phase at most `polls` times. The phase
+    // advances only when the copy has landed, so a wait that gave up can be
+    // followed by drain() on the same phase.
+    __device__ bool wait(uint32_t polls) {
         uint32_t done = 0;
-        for (uint32_t it = 0; it < (1u << 22) && !done; it++) {
+        for (uint32_t it = 0; it < polls && !done; it++) {
             asm volatile(
                 "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
                 : "=r"(done)
                 : "r"(smem_u32(bar)), "r"(phase)
                 : "memory");
         }
-        phase ^= 1u;
         __syncwarp();
-        return __all_sync(0xffffffffu, done != 0);
+        const bool ok = __all_sync(0xffffffffu, done != 0);
+        if (ok) phase ^= 1u;
+        return ok;
     }
+    // After a wait that gave up: wait for the same copy with the full bound,
+    // so that it lands before its shared memory is reused or the CTA exits.
+    // False when it still has not landed; the CTA must then issue no further
+    // copy through this barrier (its phase is unknown).
+    __device__ bool drain() { return wait(kWaitPolls); }
 };
+
+// Every job a CTA pops after its stager failed to drain reports a timeout
+// without touching shared memory, so no stream of the batch is left without
+// a status.
+__device__ __forceinline__ void mark_timeout(DecStream &S) {
+    if ((threadIdx.x & 31) == 0) S.status = FQXV_RANS_E_TIMEOUT;
+    __syncwarp();
+}
 
 // Renorm-word ring: 4 segments of 512 bytes of the word region (16-byte
 // aligned chunks, so a segment is one 16-byte load per lane). Segment q holds
@@ -504,7 +521,7 @@ __device__ __forceinline__ bool o0_general_round(uint32_t &x, const uint32_t *__
 __global__ void __launch_bounds__(32)
     dec_o0_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
-                  uint8_t *__restrict__ dst, int *__restrict__ queue) {
+                  uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t first_polls) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
     const int lane = threadIdx.x;
@@ -512,17 +529,22 @@ __global__ void __launch_bounds__(32)
     uint32_t *P = reinterpret_cast<uint32_t *>(sm);
     TableStager st;
     st.init(&bar);
+    bool stuck = false;
     for (;;) {
         const int j = pop_job(queue);
         if (j >= nlist) return;
         DecStream &S = streams[list[j]];
+        if (stuck) {
+            mark_timeout(S);
+            continue;
+        }
         st.issue(P, tbl + S.tbl_off, 16384);
         WordRing R;
         R.init(src + S.words_off, S.words_len, sm + 16384);
-        if (!st.wait()) {
-            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
-            st.wait();
-            return;
+        if (!st.wait(first_polls)) {
+            stuck = !st.drain();
+            mark_timeout(S);
+            continue;
         }
         const uint64_t n = S.n;
         const uint64_t navail = S.words_len / 2;
@@ -808,15 +830,17 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
 __global__ void __launch_bounds__(kO1Threads, 1)
     dec_o1d_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
-                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
+                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off,
+                   uint32_t first_polls) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ __align__(16) uint4 s_rows[2][kOutRows + 1];
-    __shared__ int s_job, s_ok;
+    __shared__ int s_job, s_ok, s_stuck;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t lt = lanemask_lt();
     TableStager st;
     if (warp == 0) st.init(&bar);
+    if (tid == 0) s_stuck = 0;
     __syncthreads();
     for (;;) {
         if (tid == 0) s_job = atomicAdd(queue, 1);
@@ -826,19 +850,20 @@ __global__ void __launch_bounds__(kO1Threads, 1)
         if (j >= nlist) return;
         DecStream &S = streams[list[j]];
         if (warp == 0) {
-            st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
-            const bool ok = st.wait();
-            if (!ok) {
-                if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
-                st.wait();
+            bool ok = false;
+            if (!s_stuck) {
+                st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
+                ok = st.wait(first_polls);
+                if (!ok && !st.drain() && lane == 0) s_stuck = 1;
             }
+            if (!ok) mark_timeout(S);
             if (lane == 0) s_ok = ok;
         }
         // every warp reads the words through its own ring
         WordRing R;
         R.init(src + S.words_off, S.words_len, sm + ring_off + warp * kRingBytes);
         __syncthreads();  // the table image is visible to every warp
-        if (!s_ok) return;
+        if (!s_ok) continue;
         uint8_t *out = dst + S.dst_off;
         const int tpl = (3 * S.nd + kO1Workers - 1) / kO1Workers;
         const int status = tpl <= 1 ? o1d_stream<1>(S, sm, R, s_rows, out, lt)
@@ -923,24 +948,30 @@ __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restric
 __global__ void __launch_bounds__(32)
     dec_o1s_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
-                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off) {
+                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off,
+                   uint32_t first_polls) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
     const int lane = threadIdx.x;
     const uint32_t lt = lanemask_lt();
     TableStager st;
     st.init(&bar);
+    bool stuck = false;
     for (;;) {
         const int j = pop_job(queue);
         if (j >= nlist) return;
         DecStream &S = streams[list[j]];
+        if (stuck) {
+            mark_timeout(S);
+            continue;
+        }
         st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
         WordRing R;
         R.init(src + S.words_off, S.words_len, sm + ring_off);
-        if (!st.wait()) {
-            if (lane == 0) S.status = FQXV_RANS_E_TIMEOUT;
-            st.wait();
-            return;
+        if (!st.wait(first_polls)) {
+            stuck = !st.drain();
+            mark_timeout(S);
+            continue;
         }
         const int status = o1s_stream(S, sm, R, dst + S.dst_off, lt);
         if (lane == 0) S.status = status;
@@ -1102,23 +1133,23 @@ void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint
 
 void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
-                    cudaStream_t s) {
+                    uint32_t first_polls, cudaStream_t s) {
     if (nlist <= 0 || grid <= 0) return;
     ensure_dec_attrs();
     switch (cls) {
         case kClsO0:
-            dec_o0_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
+            dec_o0_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue, first_polls);
             break;
         case kClsO1Dense:
             dec_o1d_kernel<<<grid, kO1Threads, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                        smem_bytes - kO1Warps * kRingBytes);
+                                                        smem_bytes - kO1Warps * kRingBytes, first_polls);
             break;
         case kClsO1Global:
             dec_o1g_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
             break;
         case kClsO1Small:
             dec_o1s_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                      smem_bytes - kRingBytes);
+                                                      smem_bytes - kRingBytes, first_polls);
             break;
         default:
             break;

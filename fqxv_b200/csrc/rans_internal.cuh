@@ -66,6 +66,11 @@ __host__ __device__ inline uint64_t enc_table_bytes(uint64_t n) {
     return kTblO1 + u * u * 8;
 }
 
+// Polls of an mbarrier before a decode kernel gives up on a table copy and
+// reports FQXV_RANS_E_TIMEOUT (several milliseconds; a copy lands in
+// microseconds).
+constexpr uint32_t kWaitPolls = 1u << 22;
+
 // Decode-side descriptor of one stream.
 struct DecStream {
     uint64_t src_off, src_len;   // input span
@@ -161,7 +166,7 @@ void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint
 // smem_bytes is the dynamic shared memory of the class (largest member).
 void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
-                    cudaStream_t s);
+                    uint32_t first_polls, cudaStream_t s);
 uint32_t dec_smem_bytes(int cls, int nd);
 // CTAs of a decode class that fit on one SM with `smem_bytes` of dynamic
 // shared memory (registers and static shared memory included).

@@ -19,11 +19,10 @@
 // overlaps on the GPU (different streams, or different host threads without
 // ordering) race on the array and corrupt each other's output.
 //
-// The first call on a device looks up the array's device address with that
-// device current (cudaGetSymbolAddress); make that first call before any
-// stream capture.
-#include <mutex>
-
+// Every call looks up the array's device address on the current device
+// (cudaGetSymbolAddress), so the address stays right after a
+// cudaDeviceReset reloads the module. The first call on a device may load
+// the module while doing so; make that first call before any stream capture.
 #include "rans_internal.cuh"
 
 namespace fqxv {
@@ -78,24 +77,17 @@ using namespace fqxv;
 
 namespace {
 
-std::mutex g_noalloc_mu;
-uint8_t *g_noalloc_ptr[64];
-
-// Device address of the scratch array on `dev` (looked up once per device,
-// with that device current).
-int noalloc_scratch(int dev, uint8_t **out) {
-    if (dev < 0 || dev >= 64) return FQXV_RANS_E_NO_DEVICE;
-    std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return FQXV_RANS_E_CUDA;
-        }
-        g_noalloc_ptr[dev] = static_cast<uint8_t *>(p);
+// Device address of the scratch array on the current device. The lookup is
+// repeated on every call: a cached address would go stale when
+// cudaDeviceReset unloads the module and a later call loads it again.
+int noalloc_scratch(uint8_t **out) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return FQXV_RANS_E_CUDA;
     }
-    *out = g_noalloc_ptr[dev];
+    *out = static_cast<uint8_t *>(p);
     return FQXV_RANS_OK;
 }
 
@@ -107,13 +99,13 @@ extern "C" int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int orde
     if (order < FQXV_RANS_ORDER0 || order > FQXV_RANS_BEST_TIE1) return FQXV_RANS_E_INVALID_ARG;
     if (n > kNoAllocMaxBytes) return FQXV_RANS_E_TOO_LARGE;
     if (dst_cap < fqxv_rans_encode_bound(n, order)) return FQXV_RANS_E_DST_TOO_SMALL;
-    int dev = 0;
+    int dev = 0;  // a current device must exist
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return FQXV_RANS_E_NO_DEVICE;
     }
     uint8_t *s = nullptr;
-    const int st = noalloc_scratch(dev, &s);
+    const int st = noalloc_scratch(&s);
     if (st != FQXV_RANS_OK) return st;
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
     EncBlock *B = reinterpret_cast<EncBlock *>(s + kOffBlock);

@@ -77,6 +77,10 @@ class DeviceError(Error):
 
 
 MALFORMED = {1, 2, 3, 4, 5, 6, 7, 8}
+# Statuses a batch call reports per stream (the call itself succeeded):
+# the Malformed kinds and FQXV_RANS_E_TIMEOUT (a bounded device wait gave up).
+TIMEOUT = 21
+STREAM_STATUSES = MALFORMED | {TIMEOUT}
 
 
 def lib_path() -> str:

@@ -225,20 +225,27 @@ int fqxv_rans_server_stats(fqxv_rans_server *server, uint64_t *completed, uint64
  * must hold fqxv_rans_encode_bound(n, order) bytes; its length goes to
  * *out_len. Work is queued on `stream` (a cudaStream_t, 0 = legacy default) and
  * the call returns once it is done. All calls share the array: calls whose
- * work overlaps on the GPU race and corrupt each other. The first call on a
- * device looks up the array's address; make it before any stream capture. */
+ * work overlaps on the GPU race and corrupt each other. Every call looks up
+ * the array's address on the current device (so it stays valid across a
+ * cudaDeviceReset); the first call on a device may load the library's device
+ * code while doing so, so make it before any stream capture. */
 int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int order, uint8_t *d_dst, size_t dst_cap,
                              size_t *out_len, void *stream);
 
 /* ---- per-stage device timing -------------------------------------------
  * When enabled, every kernel launch of a context is bracketed by CUDA events
  * on the context's stream and its duration accumulated per stage. Launch
- * counts are kept whether or not timing is on. */
+ * counts are kept whether or not timing is on. Launches of one stage may run
+ * side by side on several CUDA streams (the decode groups of a batch), so
+ * `ms` (the sum of launch durations) can exceed the time the stage took;
+ * `wall_ms` is that time: per call, from the stage's first launch start to
+ * its last launch end, summed over calls. */
 typedef struct fqxv_rans_stage_stat {
     char name[24];
     uint64_t launches;
     double ms;
     uint64_t bytes;   /* algorithmic bytes (input read + output written) of those launches */
+    double wall_ms;
 } fqxv_rans_stage_stat;
 
 int fqxv_rans_ctx_set_profiling(fqxv_rans_ctx *ctx, int on);

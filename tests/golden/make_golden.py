@@ -36,7 +36,9 @@ Layouts walked (all little-endian):
   `put_stream` rule keeps order-1 on a tie).
 
 Run here (where the reference tree is mounted):
-    python tests/golden/make_golden.py /root/reference/crates/fqxv/tests/fixtures
+    python tests/golden/make_golden.py <reference checkout>/crates/fqxv/tests/fixtures
+
+The fixtures directory can also be given as FQXV_FIXTURES in the environment.
 """
 
 from __future__ import annotations
@@ -229,4 +231,7 @@ def main(fixture_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/crates/fqxv/tests/fixtures")
+    fixtures = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FQXV_FIXTURES")
+    if not fixtures:
+        sys.exit("usage: %s <reference checkout>/crates/fqxv/tests/fixtures (or FQXV_FIXTURES=...)" % sys.argv[0])
+    main(fixtures)

@@ -11,7 +11,9 @@ block payloads `[24 digests][u32 n_reads]([u32 len][bytes]) x 3`, names
 first; reorder layout names frames).
 
 Run here (where the reference tree is mounted):
-    python tests/golden/make_names_golden.py /root/reference/crates/fqxv/tests/fixtures
+    python tests/golden/make_names_golden.py <reference checkout>/crates/fqxv/tests/fixtures
+
+The fixtures directory can also be given as FQXV_FIXTURES in the environment.
 """
 
 from __future__ import annotations
@@ -87,4 +89,7 @@ def main(fixture_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/crates/fqxv/tests/fixtures")
+    fixtures = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FQXV_FIXTURES")
+    if not fixtures:
+        sys.exit("usage: %s <reference checkout>/crates/fqxv/tests/fixtures (or FQXV_FIXTURES=...)" % sys.argv[0])
+    main(fixtures)

@@ -66,6 +66,86 @@ def test_normalize_random_histograms(orc):
         _check_sum(orc, c)
 
 
+def _normalize_restated(counts):
+    """Pure-Python restatement of `normalize` (crates/fqxv-rans/src/model.rs:213-264),
+    written independently of the C oracle: floor(c * 4096 / total) with a
+    minimum of 1; max_s = the first symbol with the strictly largest f; a
+    positive residual all goes to max_s; a negative one drains max_s down to 1
+    and re-picks the first symbol whose f is strictly the largest above 1."""
+    counts = [int(c) for c in counts]
+    total = sum(counts)
+    freq = [0] * 256
+    if total == 0:
+        return freq
+    fsum, max_s, max_f = 0, 0, 0
+    for s in range(256):
+        if counts[s] == 0:
+            continue
+        f = max(1, counts[s] * 4096 // total)
+        freq[s] = f
+        fsum += f
+        if f > max_f:
+            max_f, max_s = f, s
+    diff = 4096 - fsum
+    while diff != 0:
+        if diff > 0:
+            freq[max_s] += diff
+            diff = 0
+        else:
+            take = min(max(freq[max_s] - 1, 0), -diff)
+            freq[max_s] -= take
+            diff += take
+            if diff != 0:
+                nm, nf = None, 1
+                for s in range(256):
+                    if freq[s] > nf:
+                        nf, nm = freq[s], s
+                max_s = nm
+    return freq
+
+
+def drain_histograms(rng, count):
+    """Histograms whose floor frequencies overshoot 4096, so normalisation
+    takes the negative-residual path: a few large buckets (often tied, so the
+    re-pick's lowest-index rule decides) and many singletons."""
+    out = []
+    c = np.zeros(256, np.uint32)
+    c[:56] = 10_000
+    c[56:] = 1                  # 56 x 73 + 200 x 1 = 4288: diff = -192, three buckets drained
+    out.append(c)
+    for _ in range(count):
+        c = np.zeros(256, np.uint32)
+        big = int(rng.integers(1, 40))
+        small = int(rng.integers(100, 257 - big))
+        idx = rng.permutation(256)
+        c[idx[:big]] = rng.integers(500, 50_000, big) if rng.random() < 0.5 else int(rng.integers(500, 50_000))
+        c[idx[big:big + small]] = rng.integers(1, 3, small)
+        out.append(c)
+    return out
+
+
+def test_normalize_negative_residual_matches_restatement(orc):
+    rng = np.random.default_rng(11)
+    drained = 0
+    for c in drain_histograms(rng, 400):
+        want = _normalize_restated(c)
+        got = [int(v) for v in orc.normalize(c)]
+        assert got == want
+        floor = [max(1, int(v) * 4096 // int(c.sum())) if v else 0 for v in c]
+        drained += sum(floor) > 4096
+    assert drained > 300      # the crafted cases really take the drain path
+
+
+def test_normalize_random_matches_restatement(orc):
+    rng = np.random.default_rng(12)
+    for _ in range(300):
+        k = int(rng.integers(1, 257))
+        c = np.zeros(256, np.uint32)
+        idx = rng.choice(256, k, replace=False)
+        c[idx] = rng.integers(1, 1 << int(rng.integers(1, 24)), k)
+        assert [int(v) for v in orc.normalize(c)] == _normalize_restated(c)
+
+
 def test_reciprocal_and_magic_match_division(orc):
     L = orc.lib()
     L.orc_check_apply_sweep.restype = ctypes.c_size_t
