@@ -223,6 +223,78 @@ class Codec:
             rans.raise_for(st)
         return locs, status
 
+    # ---- extended stream format (include/fqxv_rans_x_gpu.h) ----------------
+
+    def _x_setup(self):
+        L = self._lib
+        if not getattr(L, "_x_ready", False):
+            vp = ctypes.c_void_p
+            L.fqxv_rans_x_encode_bound.restype = ctypes.c_uint64
+            L.fqxv_rans_x_encode_bound.argtypes = [vp, ctypes.c_size_t]
+            L.fqxv_rans_x_encode_batch.argtypes = [vp, vp, vp, ctypes.c_size_t, ctypes.c_int, vp, ctypes.c_uint64,
+                                                   vp, vp]
+            L.fqxv_rans_x_decode_batch.argtypes = [vp, vp, vp, ctypes.c_size_t, vp, vp, vp, vp]
+            L._x_ready = True
+        return L
+
+    def x_encode_batch(self, d_src, spans, flags: int, d_dst=None):
+        """Extended-format streams of the blocks `spans` of d_src with
+        transform `flags` (or 0x40: the selection). Returns (d_dst,
+        out_spans, choice)."""
+        import torch
+
+        L = self._x_setup()
+        s = _spans(spans)
+        nb = len(s)
+        if d_dst is None:
+            d_dst = torch.empty(max(L.fqxv_rans_x_encode_bound(s.ctypes.data, nb), 1), dtype=torch.uint8,
+                                device=d_src.device)
+        out = np.zeros((nb, 2), dtype=np.uint64)
+        choice = np.zeros(nb, dtype=np.int32)
+        rans.raise_for(L.fqxv_rans_x_encode_batch(self._h, d_src.data_ptr(), s.ctypes.data, nb, int(flags),
+                                                  d_dst.data_ptr(), d_dst.numel(), out.ctypes.data,
+                                                  choice.ctypes.data))
+        return d_dst, out, choice
+
+    def x_decode_batch(self, d_src, spans, out_spans, d_dst=None, raise_on_error: bool = True):
+        """Decode extended (or reference) streams; returns (d_dst, out_lens, status)."""
+        import torch
+
+        L = self._x_setup()
+        s = _spans(spans)
+        o = _spans(out_spans)
+        nb = len(s)
+        if d_dst is None:
+            need = int((o[:, 0] + o[:, 1]).max()) if nb else 1
+            d_dst = torch.empty(max(need, 1), dtype=torch.uint8, device=d_src.device)
+        lens = np.zeros(nb, dtype=np.uint64)
+        status = np.zeros(nb, dtype=np.int32)
+        st = L.fqxv_rans_x_decode_batch(self._h, d_src.data_ptr(), s.ctypes.data, nb, d_dst.data_ptr(),
+                                        o.ctypes.data, lens.ctypes.data, status.ctypes.data)
+        if st and (raise_on_error or st not in rans.STREAM_STATUSES):
+            rans.raise_for(st)
+        return d_dst, lens, status
+
+    # ---- launch shapes (fqxv_rans_ctx_set_param) ----------------------------
+
+    def set_param(self, name: str, value: int) -> None:
+        L = self._lib
+        L.fqxv_rans_ctx_set_param.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64]
+        rans.raise_for(L.fqxv_rans_ctx_set_param(self._h, name.encode(), int(value)))
+
+    def get_param(self, name: str) -> int:
+        L = self._lib
+        L.fqxv_rans_ctx_get_param.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]
+        v = ctypes.c_int64(0)
+        rans.raise_for(L.fqxv_rans_ctx_get_param(self._h, name.encode(), ctypes.byref(v)))
+        return int(v.value)
+
+    def tuning_source(self) -> str:
+        L = self._lib
+        L.fqxv_rans_ctx_tuning_source.argtypes = [ctypes.c_void_p]
+        L.fqxv_rans_ctx_tuning_source.restype = ctypes.c_char_p
+        return L.fqxv_rans_ctx_tuning_source(self._h).decode()
+
     # ---- per-stage timing ---------------------------------------------------
 
     def set_profiling(self, on: bool) -> None:

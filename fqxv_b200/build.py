@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libfqxv_rans_gpu.so")
 SOURCES = ["rans_encode.cu", "rans_decode.cu", "rans_capi.cu", "rans_noalloc.cu", "rans_server.cu",
-           "frame_kernels.cu", "frame_capi.cu", "tok_capi.cu", "streams_capi.cu",
+           "rans_x.cu", "rans_tuning.cu", "frame_kernels.cu", "frame_capi.cu", "tok_capi.cu", "streams_capi.cu",
            "perm_capi.cu"]
 HEADERS = ["rans_internal.cuh", "rans_common.cuh", "rans_ctx.cuh", "frame_internal.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -13,6 +14,7 @@
 
 #include "../../include/fqxv_streams_gpu.h"
 #include "../../include/fqxv_rans_gpu_testing.h"
+#include "../../include/fqxv_rans_x_gpu.h"
 #include "../../include/fqxv_tok_gpu.h"
 #include "frame_internal.cuh"
 #include "rans_ctx.cuh"
@@ -119,8 +121,9 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     // model and read by the encode
     uint64_t src_end = 0;
     for (size_t i = 0; i < nb; i++) src_end = std::max<uint64_t>(src_end, blocks[i].offset + blocks[i].length);
-    if (o1) CK(ctx->e_keys.ensure(2 * (src_end + 16), s));
-    uint16_t *dK = o1 ? ctx->e_keys.as<uint16_t>() : nullptr;
+    const bool keyed = o1 && ctx->enc_keys;
+    if (keyed) CK(ctx->e_keys.ensure(2 * (src_end + 16), s));
+    uint16_t *dK = keyed ? ctx->e_keys.as<uint16_t>() : nullptr;
     CK(ctx->e_misc.ensure((2 + nb) * 16, s));
     // Stage descriptors through pinned memory, one copy per array.
     const size_t szb = nb * sizeof(EncBlock), szo = nb * 4, szj = jobs.size() * sizeof(EncJob);
@@ -143,7 +146,7 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     uint8_t *dT = ctx->e_tbl.as<uint8_t>();
     uint16_t *dW = ctx->e_words.as<uint16_t>();
     uint32_t *dH = ctx->e_hist.as<uint32_t>();
-    const int run_grid = ctx->sms * 16;
+    const int run_grid = ctx->sms * (int)ctx->tune.enc_run_ctas_per_sm;
     if (persistent) {
         cudaEvent_t t0;
         if (nlarge) {
@@ -285,19 +288,32 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             if (d.cls == kClsO0) return 0;
             if (d.cls == kClsO1Global) return kGroups - 1;
             if (d.cls != kClsO1Dense) return -1;
-            return d.nd <= kSmallMaxNd ? 1 : d.nd <= 15 ? 2 : d.nd <= 31 ? 3 : 4;
+            if (d.nd <= kSmallMaxNd) return 1;
+            return d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_small   ? 2
+                   : d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_large ? 3
+                                                                         : 4;
         };
         std::vector<uint32_t> lists[kGroups];
-        uint32_t smem[kGroups] = {};
+        uint32_t tmax[kGroups] = {};
         uint64_t cbytes[kGroups] = {};
         uint64_t maxn[kGroups] = {};
         for (uint32_t i : ord) {
             const int g = group_of(ps[i]);
             if (g < 0) continue;
             lists[g].push_back(i);
-            smem[g] = std::max(smem[g], dec_smem_bytes(g == 1 ? kClsO1Small : ps[i].cls, ps[i].nd));
+            tmax[g] = std::max(tmax[g], ps[i].tbl_bytes);
             cbytes[g] += ps[i].src_len + ps[i].n;
             maxn[g] = std::max<uint64_t>(maxn[g], ps[i].n);
+        }
+        int gcls[kGroups];
+        uint32_t smem[kGroups];
+        const int64_t four_max = ctx->tune.o1_four_max_streams < 0 ? ctx->sms : ctx->tune.o1_four_max_streams;
+        for (int g = 0; g < kGroups; g++) {
+            if (g == 0) gcls[g] = kClsO0;
+            else if (g == kGroups - 1) gcls[g] = kClsO1Global;
+            else if (g == 1) gcls[g] = kClsO1Small;
+            else gcls[g] = (int64_t)lists[g].size() < four_max ? kClsO1Dense : kClsO1Wide;
+            smem[g] = dec_smem_bytes(gcls[g], tmax[g]);
         }
         // Groups are launched longest first -- by the serial time of their
         // largest stream (rounds x cycles per round: ~620 for order-1,
@@ -325,13 +341,18 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             const int g = glaunch[gi];
             const size_t m = lists[g].size();
             if (!m) continue;
-            const int cls = g == 0 ? kClsO0 : g == kGroups - 1 ? kClsO1Global : g == 1 ? kClsO1Small : kClsO1Dense;
-            const int stage = g == 0 ? kStDecO0 : g == kGroups - 1 ? kStDecO1Global : g == 1 ? kStDecO1Small
-                                                                                              : kStDecO1Dense;
+            const int cls = gcls[g];
+            const int stage = cls == kClsO0 ? kStDecO0 : cls == kClsO1Global ? kStDecO1Global
+                              : cls == kClsO1Small ? kStDecO1Small : cls == kClsO1Wide ? kStDecO1Wide
+                                                                                         : kStDecO1Dense;
             cudaStream_t as = ctx->aux[g];
             CK(cudaStreamWaitEvent(as, ctx->ev_fork, 0));
             int per_sm = dec_blocks_per_sm(cls, smem[g]);
-            per_sm = std::max(1, std::min(per_sm, cls == kClsO1Dense ? 8 : 32));
+            const Tuning &T = ctx->tune;
+            const int64_t cap = cls == kClsO0 ? T.cta_cap_o0 : cls == kClsO1Small ? T.cta_cap_o1_small
+                                : cls == kClsO1Wide ? T.cta_cap_o1_wide : cls == kClsO1Dense ? T.cta_cap_o1_four
+                                                                                            : T.cta_cap_o1_global;
+            per_sm = std::max(1, std::min<int>(per_sm, (int)cap));
             if (persistent) {
                 const int grid = (int)std::min<size_t>(m, (size_t)ctx->sms * per_sm);
                 cudaEvent_t t0 = ctx->timer.begin(as);
@@ -343,7 +364,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
                     CK(cudaMemsetAsync(queue + 4 * g, 0, 4, as));
                     cudaEvent_t t0 = ctx->timer.begin(as);
                     launch_dec_run(cls, d_src, dS, dl + base[g] + j, 1, dT, d_dst, queue + 4 * g, 1,
-                                   dec_smem_bytes(cls, ps[lists[g][j]].nd), ctx->first_polls, as);
+                                   dec_smem_bytes(cls, ps[lists[g][j]].tbl_bytes), ctx->first_polls, as);
                     ctx->timer.end(stage, t0, as);
                 }
             }
@@ -415,6 +436,7 @@ const char *fqxv_rans_status_message(int status) {
         case FQXV_RANS_E_ALLOC: return "rANS output length too large to allocate";
         case FQXV_RANS_E_BOUND: return "rANS output length exceeds caller bound";
         case FQXV_RANS_E_TRUNCATED_RENORM: return "truncated renorm stream";
+        case FQXV_RANS_E_X_MALFORMED: return "malformed extended stream";
         case FQXV_RANS_E_INVALID_ARG: return "invalid argument";
         case FQXV_RANS_E_DST_TOO_SMALL: return "destination buffer too small";
         case FQXV_RANS_E_CUDA: return "CUDA error";
@@ -468,6 +490,15 @@ int fqxv_rans_ctx_create(int device, fqxv_rans_ctx **out) {
     auto *c = new fqxv_rans_ctx();
     c->device = device;
     c->sms = sm_count(device);
+    tuning_load(c->tune, device);
+    // FQXV_RANS_O1_DECODER=wide|four pins the decoder of wide order-1
+    // alphabets (for measurements); anything else keeps the table's rule.
+    if (const char *e = std::getenv("FQXV_RANS_O1_DECODER")) {
+        if (!std::strcmp(e, "wide")) c->tune.o1_four_max_streams = 0;
+        else if (!std::strcmp(e, "four")) c->tune.o1_four_max_streams = 1 << 30;
+    }
+    // FQXV_RANS_ENC_KEYS=0: order-1 encode without the per-position key array.
+    if (const char *e = std::getenv("FQXV_RANS_ENC_KEYS")) c->enc_keys = std::strcmp(e, "0") != 0;
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; i < kGroups && ok; i++)
@@ -489,6 +520,7 @@ void fqxv_rans_ctx_destroy(fqxv_rans_ctx *ctx) {
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->for_each_buf([](DevBuf &b) { b.release(); });
+    x_release(ctx);
     ctx->h_stage.release();
     ctx->h_io.release();
     ctx->timer.release();
@@ -617,6 +649,25 @@ int fqxv_rans_ctx_set_profiling(fqxv_rans_ctx *ctx, int on) {
     return FQXV_RANS_OK;
 }
 
+int fqxv_rans_ctx_set_param(fqxv_rans_ctx *ctx, const char *name, int64_t value) {
+    if (!ctx || !name) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    const int st = tuning_set(ctx->tune, name, value);
+    if (st == FQXV_RANS_OK)
+        for (auto *c : ctx->sub) tuning_set(c->tune, name, value);
+    return st;
+}
+
+int fqxv_rans_ctx_get_param(fqxv_rans_ctx *ctx, const char *name, int64_t *value) {
+    if (!ctx || !name || !value) return FQXV_RANS_E_INVALID_ARG;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    return tuning_get(ctx->tune, name, *value);
+}
+
+const char *fqxv_rans_ctx_tuning_source(fqxv_rans_ctx *ctx) {
+    return ctx && !ctx->tune.source.empty() ? ctx->tune.source.c_str() : "";
+}
+
 int fqxv_rans_ctx_test_set_wait_polls(fqxv_rans_ctx *ctx, uint32_t polls) {
     if (!ctx) return FQXV_RANS_E_INVALID_ARG;
     std::lock_guard<std::mutex> g(ctx->mu);
@@ -718,6 +769,7 @@ int ensure_subs(fqxv_rans_ctx *ctx, size_t k) {
         const int st = fqxv_rans_ctx_create(ctx->device, &c);
         if (st != FQXV_RANS_OK) return st;
         c->first_polls = ctx->first_polls;
+        c->tune = ctx->tune;
         ctx->sub.push_back(c);
     }
     return FQXV_RANS_OK;

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "rans_internal.cuh"
@@ -75,12 +76,34 @@ constexpr int kGroups = 6;  // decode launch groups
 
 enum Stage {
     kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
-    kStDecO1Small, kStCrcPlan, kStCrc, kStFrameCopy, kStFrameWalk, kStages
+    kStDecO1Small, kStDecO1Wide, kStCrcPlan, kStCrc, kStFrameCopy, kStFrameWalk, kStages
 };
 const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan", "enc_pack",
                                           "dec_parse", "dec_o0", "dec_o1_dense", "dec_o1_global",
-                                          "dec_o1_small", "crc_plan", "crc32c", "frame_copy_crc",
-                                          "frame_walk"};
+                                          "dec_o1_small", "dec_o1_wide", "crc_plan", "crc32c",
+                                          "frame_copy_crc", "frame_walk"};
+
+// Launch-shape parameters of a context (rans_tuning.cu): defaults are the
+// library's run-time rules; a tuning table measured on the device replaces
+// them.
+struct Tuning {
+    // Order-1 streams of more than kSmallMaxNd symbols with shared-memory
+    // tables: a launch group of fewer than this many goes to the four-warp
+    // decoder (one stream per SM), larger groups to the one-warp decoder
+    // (several per SM). -1: the SM count.
+    int64_t o1_four_max_streams = -1;
+    // CTAs per SM of each decode class, at most (the occupancy API bounds it too)
+    int64_t cta_cap_o0 = 32, cta_cap_o1_small = 32, cta_cap_o1_wide = 32, cta_cap_o1_four = 8,
+            cta_cap_o1_global = 32;
+    // table-image sizes cutting dense order-1 streams into launch groups
+    int64_t dense_edge_small = 40 << 10, dense_edge_large = 80 << 10;
+    // encode kernel grid, CTAs per SM
+    int64_t enc_run_ctas_per_sm = 16;
+    std::string source;  // the table file applied (empty: defaults)
+};
+int tuning_set(Tuning &t, const char *key, int64_t value);
+int tuning_get(const Tuning &t, const char *key, int64_t &value);
+void tuning_load(Tuning &t, int device);
 
 // CUDA-event brackets around each kernel launch on the context's stream.
 // Durations are collected after the call's final synchronisation. Launches of
@@ -196,6 +219,8 @@ void *mapped_device_ptr(const void *h);
 }  // namespace fqxv
 
 namespace fqxv {
+// Frees a context's extended-format arenas (rans_x.cu).
+void x_release(fqxv_rans_ctx *ctx);
 // fqxv_rans_encode_batch / fqxv_rans_decode_batch (persistent form) for
 // callers that already hold ctx->mu and have the context's device current.
 int encode_batch_locked(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks, size_t nb, int mode,
@@ -227,6 +252,14 @@ struct fqxv_rans_ctx {
     // the full bound follows a wait that gives up). Only the test-only
     // setter in fqxv_rans_gpu_testing.h lowers it.
     uint32_t first_polls = fqxv::kWaitPolls;
+    fqxv::Tuning tune;
+    // Order-1 encode: the model kernel stores each position's table index
+    // (u16) for the encode kernel to read back, instead of the encode
+    // kernel deriving it from the byte and its predecessor.
+    bool enc_keys = true;
+    // arenas of the extended-format calls (rans_x.cu), created on first use
+    // and freed by fqxv::x_release
+    void *xb = nullptr;
     // host-buffer batches cut into chunks run one chunk per sub-context
     std::vector<fqxv_rans_ctx *> sub;
     template <class F>

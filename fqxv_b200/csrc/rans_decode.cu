@@ -44,8 +44,9 @@ __global__ void __launch_bounds__(kParseThreads)
     __shared__ uint8_t ctxlist[256];  // present-table index -> raw context
     __shared__ uint8_t dmap[256];     // raw byte -> dense index (0xFF not in D)
     __shared__ uint8_t symseen[256];
-    __shared__ __align__(16) uint8_t smap[kParseThreads / 32][kTotFreq];  // per warp: slot -> dense symbol
-    __shared__ int s_k, s_nd, s_bad;
+    __shared__ uint16_t s_col[kTotFreq];  // dense format: column index of every slot
+    __shared__ uint32_t s_bnd[kTotFreq / 32];   // dense format: boundary bitmap over the slots
+    __shared__ int s_k, s_nd, s_bad, s_ncol;
     __shared__ uint8_t s_badst[256];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
@@ -197,48 +198,84 @@ __global__ void __launch_bounds__(kParseThreads)
                 }
                 __syncthreads();
                 const int nd = s_nd;
-                if (nd <= kDenseMax) {
+                // f and exclusive cum of the 8 symbols lane owns in table t
+                auto read_row = [&](int t, uint32_t f[8], uint32_t cum[8]) {
+                    const uint64_t at = kHdr + kO1Bitmap + kO1Table * (uint64_t)t;
+                    uint32_t run = 0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        f[k] = (uint32_t)p[at + 16 * lane + 2 * k] | ((uint32_t)p[at + 16 * lane + 2 * k + 1] << 8);
+                        cum[k] = run;
+                        run += f[k];
+                    }
+                    const uint32_t base = warp_incl_scan(run) - run;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) cum[k] += base;
+                };
+                bool dense = nd <= kDenseMax;
+                if (dense) {
+                    // Boundaries: every slot where a present symbol of some
+                    // context starts (slot 0 always, so a column exists even
+                    // without any table); the column of a slot is the number
+                    // of boundaries at or below it, minus one.
+                    if (tid < (int)(kTotFreq / 32)) s_bnd[tid] = tid == 0 ? 1u : 0u;
+                    __syncthreads();
+                    for (int t = warp; t < K; t += kParseThreads / 32) {
+                        uint32_t f[8], cum[8];
+                        read_row(t, f, cum);
+#pragma unroll
+                        for (int k = 0; k < 8; k++)
+                            if (f[k]) atomicOr(&s_bnd[cum[k] >> 5], 1u << (cum[k] & 31));
+                    }
+                    __syncthreads();
+                    const uint32_t w = tid < (int)(kTotFreq / 32) ? s_bnd[tid] : 0u;
+                    const uint32_t c = __popc(w);
+                    const uint32_t incl = warp_incl_scan(c);
+                    if (lane == 31) wsum[warp] = incl;
+                    __syncthreads();
+                    if (tid < (int)(kTotFreq / 32)) {
+                        uint32_t run = incl - c;
+                        for (int q = 0; q < warp; q++) run += wsum[q];
+                        for (int b = 0; b < 32; b++) {
+                            run += (w >> b) & 1u;
+                            s_col[tid * 32 + b] = (uint16_t)(run - 1);
+                        }
+                    }
+                    if (tid == 0) {
+                        uint32_t tot = 0;
+                        for (int q = 0; q < kParseThreads / 32; q++) tot += wsum[q];
+                        s_ncol = (int)tot;
+                    }
+                    __syncthreads();
+                    dense = dense_table_bytes(nd, (uint32_t)s_ncol) <= kDenseImageMax;
+                }
+                if (dense) {
+                    const uint32_t ncol = (uint32_t)s_ncol;
                     const int dead = nd;
                     const int stride = nd + 1;
-                    uint8_t *CT = T;
-                    uint32_t *FC = reinterpret_cast<uint32_t *>(T + dense_chain_bytes(nd));
-                    uint8_t *DS = T + dense_chain_bytes(nd) + dense_fc_bytes(nd);
-                    // Rows of dense indices without a table (and DEAD) map every
-                    // slot to DEAD; the FC table starts zeroed.
-                    for (int b = 0; b <= 256; b++) {
-                        int d;
-                        if (b < 256) {
-                            if (dmap[b] == 0xff || ctxmap[b] != 0xff) continue;
-                            d = dmap[b];
-                        } else {
-                            d = dead;
-                        }
-                        uint32_t *row = reinterpret_cast<uint32_t *>(CT + (uint64_t)d * kChainStride);
-                        const uint32_t v = 0x01010101u * (uint32_t)dead;
-                        for (int i = tid; i < (int)kChainStride / 4; i += blockDim.x) row[i] = v;
-                    }
+                    const uint32_t cs = dense_col_stride(nd);
+                    uint16_t *M = reinterpret_cast<uint16_t *>(T);
+                    uint32_t *FC = reinterpret_cast<uint32_t *>(T + kDenseM);
+                    uint8_t *DS = T + kDenseM + dense_fc_bytes(nd);
+                    uint8_t *COL = T + dense_col_off(nd);
+                    // Every column entry starts DEAD (rows of contexts without
+                    // a table, the DEAD row, padding); FC starts zeroed.
+                    const uint32_t deadw = 0x01010101u * (uint32_t)dead;
+                    for (uint32_t i = tid; i < ncol * cs / 4; i += blockDim.x)
+                        reinterpret_cast<uint32_t *>(COL)[i] = deadw;
                     for (int i = tid; i < stride * stride; i += blockDim.x) FC[i] = 0;
+                    for (int i = tid; i < (int)kTotFreq; i += blockDim.x) M[i] = (uint16_t)(s_col[i] * (cs >> 4));
                     if (tid < 256 && dmap[tid] != 0xff) DS[dmap[tid]] = (uint8_t)tid;
                     __syncthreads();
-                    // Pass 2: chain rows and FC rows of the present contexts,
-                    // one warp per context: the warp paints each symbol's slot
-                    // range [cum, cum + f) into its shared slot map, then
-                    // stores the map as the context's chain row.
-                    uint8_t *sm = smap[warp];
+                    // One warp per present context: its FC row, and its row
+                    // of every column -- the columns of a symbol's slot range
+                    // [cum, cum + f) are s_col[cum] .. s_col[cum + f - 1].
                     for (int t = warp; t < K; t += kParseThreads / 32) {
-                        const uint64_t at = kHdr + kO1Bitmap + kO1Table * (uint64_t)t;
                         const int dc = dmap[ctxlist[t]];
-                        uint32_t f[8], cum[8], run = 0;
+                        uint32_t f[8], cum[8];
+                        read_row(t, f, cum);
 #pragma unroll
                         for (int k = 0; k < 8; k++) {
-                            f[k] = (uint32_t)p[at + 16 * lane + 2 * k] | ((uint32_t)p[at + 16 * lane + 2 * k + 1] << 8);
-                            cum[k] = run;
-                            run += f[k];
-                        }
-                        const uint32_t base = warp_incl_scan(run) - run;
-#pragma unroll
-                        for (int k = 0; k < 8; k++) {
-                            cum[k] += base;
                             const uint32_t sym = lane * 8 + k;
                             if (f[k]) FC[dc * stride + dmap[sym]] = (f[k] << kScaleBits) | cum[k];
                         }
@@ -251,21 +288,17 @@ __global__ void __launch_bounds__(kParseThreads)
                                 const uint32_t c0 = __shfl_sync(0xffffffffu, cum[k], src);
                                 const uint32_t fk = __shfl_sync(0xffffffffu, f[k], src);
                                 const uint8_t dv = dmap[src * 8 + k];
-                                for (uint32_t i = lane; i < fk; i += 32) sm[c0 + i] = dv;
+                                const uint32_t j1 = s_col[c0 + fk - 1];
+                                for (uint32_t j = s_col[c0] + lane; j <= j1; j += 32) COL[j * cs + dc] = dv;
                             }
                         }
-                        __syncwarp();
-                        uint32_t *row = reinterpret_cast<uint32_t *>(CT + (uint64_t)dc * kChainStride);
-                        const uint32_t *sm32 = reinterpret_cast<const uint32_t *>(sm);
-                        for (int i = lane; i < (int)kTotFreq / 4; i += 32) row[i] = sm32[i];
-                        __syncwarp();
                     }
                     __syncthreads();
                     if (tid == 0) {
                         S.cls = kClsO1Dense;
                         S.nd = nd;
                         S.start = dmap[0] != 0xff ? dmap[0] : dead;
-                        S.tbl_bytes = dense_table_bytes(nd);
+                        S.tbl_bytes = dense_table_bytes(nd, ncol);
                     }
                 } else {
                     if (tid < 256) T[kDecCtxMap + tid] = ctxmap[tid];
@@ -615,10 +648,13 @@ __global__ void __launch_bounds__(32)
 // Decode one order-1 stream whose dense tables are in shared memory, with
 // four warps (kO1Warps) per stream.
 //
-// Per round, the context chain d_i = chain[d_{i-1}][slot_i] of the 32 lanes
-// is resolved in four segments of eight: segment 0 from the known incoming
+// Per round, the context chain d_i = col(slot_i)[d_{i-1}] of the 32 lanes is
+// resolved in four segments of eight: segment 0 from the known incoming
 // context, segments 1-3 for every possible incoming context at once, then
-// three dependent lookups pick the real rows. Every warp holds its own copy
+// three dependent lookups pick the real rows. A lane turns its slot into the
+// byte offset of the slot's column once per round (one lookup in M), so each
+// chain step is one byte load from a column: the steps of all chains of a
+// segment read the same column (at most 48 bytes), not a row per context. Every warp holds its own copy
 // of the 32 states, the word position and the incoming context, and runs the
 // same renormalisation on the same words (from its own word ring), so the
 // copies never diverge and one barrier per round suffices: each thread runs
@@ -635,9 +671,9 @@ __device__ __forceinline__ void named_bar(int id) {
 }
 
 // The rounds of one order-1 dense stream (scalar.rs:202-215), shared by the
-// 4-warp and the 1-warp decoders: `resolve(slot, d, ctx)` runs one round's
-// context chain and gives this lane's symbol and context; `store` says
-// whether this warp writes the output.
+// 4-warp and the 1-warp decoders: `resolve(slot, cb, d, ctx)` runs one
+// round's context chain and gives this lane's symbol and context; `store`
+// says whether this warp writes the output.
 //
 // Rounds that cannot run out of words (and are not the first or the partial
 // last round) take a branch-free fast path: the ring advances by predication,
@@ -645,11 +681,19 @@ __device__ __forceinline__ void named_bar(int id) {
 // run of fast rounds -- such a stream fails anyway, and a truncation cannot
 // come earlier inside those rounds. Other rounds take the careful path with
 // every check of scalar.rs:202-215 in order.
+//
+// `resolve` gets the lane's slot and the byte offset of its column (M[slot]
+// in 16-byte units, times 16). In fast rounds the next round's column is
+// found while this round renormalises: a lane that takes a word gets its
+// column with it (the column of every candidate word is looked up when the
+// window is read, and shuffled along with the word); a lane that takes none
+// looks up the column of its new value while the vote runs. So the M lookup
+// is off the chain from one round to the next.
 template <class Resolve>
 __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__restrict__ out, uint32_t lt,
-                                         const uint32_t *__restrict__ FC, const uint8_t *__restrict__ DS,
-                                         uint32_t stride, uint32_t dead, bool store, uint32_t x,
-                                         Resolve &&resolve) {
+                                         const uint16_t *__restrict__ M, const uint32_t *__restrict__ FC,
+                                         const uint8_t *__restrict__ DS, uint32_t stride, uint32_t dead, bool store,
+                                         uint32_t x, Resolve &&resolve) {
     const int lane = threadIdx.x & 31;
     const uint64_t n = S.n;
     const uint64_t navail = S.words_len / 2;
@@ -669,7 +713,7 @@ __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__r
             const bool active = i < n;
             const uint32_t slot = x & (kTotFreq - 1);
             uint32_t d, ctx;
-            resolve(slot, d, ctx);
+            resolve(slot, (uint32_t)M[slot] << 4, d, ctx);
             const uint32_t deadmask = __ballot_sync(0xffffffffu, active && d == dead);
             const int absent_at = deadmask ? __ffs(deadmask) - 1 : 32;
             const bool valid = active && lane < absent_at;
@@ -697,6 +741,7 @@ __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__r
         uint32_t adv_at = (uint32_t)((512u * (uint32_t)(R.next_seg - 3) - R.lead + 1u) / 2u);
         uint32_t sawdead = 0;
         uint8_t *op = out + r * 32 + lane;
+        uint32_t cb = (uint32_t)M[x & (kTotFreq - 1)] << 4;
         for (int64_t c = 0; c < cnt; c++) {
             // predicated one-segment ring advance (a round moves <= 64 bytes)
             const bool adv = w32 - (uint32_t)wp >= adv_at - (uint32_t)wp;
@@ -708,18 +753,23 @@ __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__r
             }
             __syncwarp();
             const uint32_t cand = R.word(w32 + lane);
+            const uint32_t cbc = (uint32_t)M[cand & (kTotFreq - 1)] << 4;
             const uint32_t slot = x & (kTotFreq - 1);
             uint32_t d, ctx;
-            resolve(slot, d, ctx);
+            resolve(slot, cb, d, ctx);
             sawdead |= d == dead;
             const uint32_t fc = FC[ctx * stride + d];
             const uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
+            const uint32_t cbv = (uint32_t)M[v & (kTotFreq - 1)] << 4;
             const bool need = v < kRansL;
             const uint32_t mask = __ballot_sync(0xffffffffu, need);
-            const uint32_t w = __shfl_sync(0xffffffffu, cand, __popc(mask & lt) & 31);
+            const uint32_t srcl = __popc(mask & lt) & 31;
+            const uint32_t w = __shfl_sync(0xffffffffu, cand, srcl);
+            const uint32_t cbw = __shfl_sync(0xffffffffu, cbc, srcl);
             if (store) *op = DS[d];
             op += 32;
             x = need ? (v << 16) | w : v;
+            cb = need ? cbw : cbv;
             w32 += __popc(mask);
         }
         wp += (uint32_t)(w32 - (uint32_t)wp);
@@ -739,13 +789,31 @@ constexpr uint32_t kDeadRow = 3 * kDenseMax;
 constexpr uint32_t kPadRow = kDeadRow + 1;
 static_assert(kPadRow <= kOutRows, "row array too small");
 
+// The parts of a dense table image in shared memory.
+struct DenseImage {
+    const uint16_t *M;     // slot -> column offset in 16-byte units
+    const uint8_t *COL;    // columns
+    const uint32_t *FC;    // (freq << 12) | cum per (context, symbol)
+    const uint8_t *DS;     // dense index -> byte
+    uint32_t stride;       // FC row stride (nd + 1)
+    uint32_t dead;
+    __device__ DenseImage(const uint8_t *sm, int nd)
+        : M(reinterpret_cast<const uint16_t *>(sm)),
+          COL(sm + dense_col_off(nd)),
+          FC(reinterpret_cast<const uint32_t *>(sm + kDenseM)),
+          DS(sm + kDenseM + dense_fc_bytes(nd)),
+          stride((uint32_t)nd + 1),
+          dead((uint32_t)nd) {}
+};
+
 template <int TPL>
 __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
                                           uint4 (*__restrict__ rows)[kOutRows + 1], uint8_t *__restrict__ out,
                                           uint32_t lt) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nd = S.nd;
-    const uint32_t dead = (uint32_t)nd;
+    const DenseImage I(sm, nd);
+    const uint32_t dead = I.dead;
     const int nspec = 3 * nd;
     // This thread's chains: lane 0 of each warp runs segment 0 (q = 0); the
     // other threads split the speculative tasks u = (seg - 1) nd + c.
@@ -760,10 +828,7 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         idx_q[q] = valid ? (uint32_t)u : kPadRow;
         nbase_q[q] = seg_q[q] * (uint32_t)nd;  // first row of the next segment
     }
-    const uint8_t *CT = sm;
-    const uint32_t stride = (uint32_t)nd + 1;
-    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
-    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
+    const uint8_t *COL = I.COL;
     const uint32_t deadw = 0x01010101u * dead;
     if (tid == 0) {
         rows[0][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
@@ -778,23 +843,23 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
 
     // One round: the chains of this thread, the barrier, then the resolved
     // symbol d and context ctx of this lane.
-    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
+    auto resolve = [&](uint32_t, uint32_t cb, uint32_t &d, uint32_t &ctx) {
         uint4 mine[TPL];
 #pragma unroll
         for (int q = 0; q < TPL; q++) {
             uint32_t sl[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, slot, 8 * seg_q[q] + k);
+            for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, cb, 8 * seg_q[q] + k);
             uint32_t dd = (q == 0 && lane == 0) ? din : c_q[q];
             uint32_t hi = 0, lo = 0;
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                dd = CT[dd * kChainStride + sl[k]];
+                dd = COL[sl[k] + dd];
                 hi = hi * 256u + dd;
             }
 #pragma unroll
             for (int k = 4; k < 8; k++) {
-                dd = CT[dd * kChainStride + sl[k]];
+                dd = COL[sl[k] + dd];
                 lo = lo * 256u + dd;
             }
             mine[q] = make_uint4(hi, lo, 16u * (dd == dead ? kDeadRow : nbase_q[q] + dd), 0u);
@@ -824,7 +889,7 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         buf ^= 1u;
     };
 
-    return o1_rounds(S, R, out, lt, FC, DS, stride, dead, warp == 0, x, resolve);
+    return o1_rounds(S, R, out, lt, I.M, I.FC, I.DS, I.stride, dead, warp == 0, x, resolve);
 }
 
 __global__ void __launch_bounds__(kO1Threads, 1)
@@ -874,49 +939,47 @@ __global__ void __launch_bounds__(kO1Threads, 1)
 }
 
 // ---------------------------------------------------------------------------
-// order-1, small alphabets (|D| <= kSmallMaxNd): one warp per stream
+// order-1, one warp per stream
 // ---------------------------------------------------------------------------
 
-// The same four segments of eight, but every chain fits in one warp: lane 0
+// Small alphabets (|D| <= kSmallMaxNd): every chain fits in one warp: lane 0
 // runs segment 0 from the known context, lanes 1..3 nd run segment s >= 1
 // from every possible incoming context (lane 1 + (s - 1) nd + c), lane 31
 // holds the DEAD row. Each row carries the lane of the row the next segment
 // continues from, so resolving a round is three dependent shuffles -- no
 // shared rows, no barrier, no copies of the states. With tables of a few
-// tens of KB, several streams share an SM.
+// KB, many streams share an SM.
 __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
                                           uint8_t *__restrict__ out, uint32_t lt) {
     const int lane = threadIdx.x & 31;
     const int nd = S.nd;
-    const uint32_t dead = (uint32_t)nd;
+    const DenseImage I(sm, nd);
+    const uint32_t dead = I.dead;
     const bool task = lane >= 1 && lane <= 3 * nd;
     const uint32_t myseg = task ? (uint32_t)(1 + (lane - 1) / nd) : 0u;
     const uint32_t myc = task ? (uint32_t)((lane - 1) % nd) : 0u;
     const uint32_t nbase = 1u + myseg * (uint32_t)nd;  // lane of the next segment's context-0 row
-    const uint8_t *CT = sm;
-    const uint32_t stride = (uint32_t)nd + 1;
-    const uint32_t *FC = reinterpret_cast<const uint32_t *>(sm + dense_chain_bytes(nd));
-    const uint8_t *DS = sm + dense_chain_bytes(nd) + dense_fc_bytes(nd);
+    const uint8_t *COL = I.COL;
     const uint32_t deadw = 0x01010101u * dead;
     uint32_t din = (uint32_t)S.start;
     const int seg = lane >> 3, pos = lane & 7;
     const uint32_t shd = 24u - 8u * (uint32_t)(pos & 3);
     const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);
 
-    auto resolve = [&](uint32_t slot, uint32_t &d, uint32_t &ctx) {
+    auto resolve = [&](uint32_t, uint32_t cb, uint32_t &d, uint32_t &ctx) {
         uint32_t sl[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, slot, 8 * myseg + k);
+        for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, cb, 8 * myseg + k);
         uint32_t dd = lane == 0 ? din : myc;
         uint32_t hi = 0, lo = 0;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            dd = CT[dd * kChainStride + sl[k]];
+            dd = COL[sl[k] + dd];
             hi = hi * 256u + dd;
         }
 #pragma unroll
         for (int k = 4; k < 8; k++) {
-            dd = CT[dd * kChainStride + sl[k]];
+            dd = COL[sl[k] + dd];
             lo = lo * 256u + dd;
         }
         uint32_t nx = dd == dead ? 31u : nbase + dd;
@@ -942,16 +1005,121 @@ __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restric
         ctx = pos == 0 ? in : ((pos <= 4 ? row_x : row_y) >> shc) & 0xffu;
         din = r3y & 0xffu;
     };
-    return o1_rounds(S, R, out, lt, FC, DS, stride, dead, true, S.states[lane], resolve);
+    return o1_rounds(S, R, out, lt, I.M, I.FC, I.DS, I.stride, dead, true, S.states[lane], resolve);
 }
 
+// Wider alphabets (kSmallMaxNd < |D| <= kDenseMax) in one warp: lane 0 runs
+// segment 0; lanes 1-10, 11-20 and 21-30 run segments 1, 2 and 3, lane i of
+// a segment following the incoming contexts i, i + 10, ... (TPL chains per
+// lane, TPL = ceil(nd / 10), interleaved so their loads overlap). All chains
+// of a lane share one segment, so a round needs eight slot shuffles per
+// lane whatever TPL is. Rows go to a double-buffered shared array and are
+// resolved after a __syncwarp with three dependent loads, as in the
+// four-warp decoder, but without its barrier or its replicated states: one
+// warp and ~30 KB of shared memory per full-range quality stream, so several
+// streams share an SM.
+constexpr int kWideLanes = 10;  // lanes per speculative segment
+
+template <int TPL>
+__device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
+                                          uint4 (*__restrict__ rows)[kOutRows + 1], uint8_t *__restrict__ out,
+                                          uint32_t lt) {
+    const int lane = threadIdx.x & 31;
+    const int nd = S.nd;
+    const DenseImage I(sm, nd);
+    const uint32_t dead = I.dead;
+    const bool worker = lane >= 1 && lane <= 3 * kWideLanes;
+    const uint32_t myseg = worker ? (uint32_t)(1 + (lane - 1) / kWideLanes) : 0u;
+    const uint32_t li = worker ? (uint32_t)((lane - 1) % kWideLanes) : 0u;
+    const uint32_t nbase = myseg * (uint32_t)nd;  // first row of the next segment
+    uint32_t c_q[TPL], idx_q[TPL];
+#pragma unroll
+    for (int q = 0; q < TPL; q++) {
+        const uint32_t c = li + kWideLanes * q;
+        const bool valid = worker && c < (uint32_t)nd;
+        c_q[q] = valid ? c : 0u;
+        idx_q[q] = valid ? (myseg - 1) * (uint32_t)nd + c : kPadRow;
+    }
+    const uint8_t *COL = I.COL;
+    const uint32_t deadw = 0x01010101u * dead;
+    if (lane == 0) {
+        rows[0][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
+        rows[1][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
+    }
+    __syncwarp();
+    uint32_t din = (uint32_t)S.start;
+    const int seg = lane >> 3, pos = lane & 7;
+    const uint32_t shd = 24u - 8u * (uint32_t)(pos & 3);
+    const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);
+    uint32_t buf = 0;
+
+    auto resolve = [&](uint32_t, uint32_t cb, uint32_t &d, uint32_t &ctx) {
+        uint32_t sl[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, cb, 8 * myseg + k);
+        uint32_t dd[TPL], hi[TPL], lo[TPL];
+#pragma unroll
+        for (int q = 0; q < TPL; q++) {
+            dd[q] = (q == 0 && lane == 0) ? din : c_q[q];
+            hi[q] = 0;
+            lo[q] = 0;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+#pragma unroll
+            for (int q = 0; q < TPL; q++) {
+                dd[q] = COL[sl[k] + dd[q]];
+                hi[q] = hi[q] * 256u + dd[q];
+            }
+        }
+#pragma unroll
+        for (int k = 4; k < 8; k++) {
+#pragma unroll
+            for (int q = 0; q < TPL; q++) {
+                dd[q] = COL[sl[k] + dd[q]];
+                lo[q] = lo[q] * 256u + dd[q];
+            }
+        }
+        uint4 *rb = rows[buf];
+#pragma unroll
+        for (int q = 0; q < TPL; q++) {
+            const uint32_t nx = 16u * (dd[q] == dead ? kDeadRow : nbase + dd[q]);
+            if (q > 0 || lane != 0) rb[idx_q[q]] = make_uint4(hi[q], lo[q], nx, 0u);
+        }
+        uint4 r0;
+        r0.x = __shfl_sync(0xffffffffu, hi[0], 0);
+        r0.y = __shfl_sync(0xffffffffu, lo[0], 0);
+        r0.z = __shfl_sync(0xffffffffu, 16u * (dd[0] == dead ? kDeadRow : nbase + dd[0]), 0);
+        __syncwarp();
+        const uint8_t *rbb = reinterpret_cast<const uint8_t *>(rb);
+        const uint4 r1 = *reinterpret_cast<const uint4 *>(rbb + r0.z);
+        const uint4 r2 = *reinterpret_cast<const uint4 *>(rbb + r1.z);
+        const uint32_t rx = seg == 0 ? r0.x : seg == 1 ? r1.x : r2.x;
+        const uint32_t ry = seg == 0 ? r0.y : seg == 1 ? r1.y : r2.y;
+        const uint32_t ine = seg == 0 ? din : seg == 1 ? (r0.y & 0xffu) : (r1.y & 0xffu);
+        const uint4 r3 = *reinterpret_cast<const uint4 *>(rbb + r2.z);
+        const uint32_t row_x = seg == 3 ? r3.x : rx;
+        const uint32_t row_y = seg == 3 ? r3.y : ry;
+        const uint32_t in = seg == 3 ? (r2.y & 0xffu) : ine;
+        d = ((pos < 4 ? row_x : row_y) >> shd) & 0xffu;
+        ctx = pos == 0 ? in : ((pos <= 4 ? row_x : row_y) >> shc) & 0xffu;
+        din = r3.y & 0xffu;
+        buf ^= 1u;
+    };
+    return o1_rounds(S, R, out, lt, I.M, I.FC, I.DS, I.stride, dead, true, S.states[lane], resolve);
+}
+
+// The two one-warp order-1 decoders: `wide` selects o1w_stream (rows in
+// shared memory, TPL chains per lane) over o1s_stream.
+template <bool kWide>
 __global__ void __launch_bounds__(32)
-    dec_o1s_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
+    dec_o1w_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
                    uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off,
                    uint32_t first_polls) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(16) uint4 s_rows[kWide ? 2 : 1][kWide ? kOutRows + 1 : 1];
     const int lane = threadIdx.x;
     const uint32_t lt = lanemask_lt();
     TableStager st;
@@ -973,11 +1141,22 @@ __global__ void __launch_bounds__(32)
             mark_timeout(S);
             continue;
         }
-        const int status = o1s_stream(S, sm, R, dst + S.dst_off, lt);
+        uint8_t *out = dst + S.dst_off;
+        int status;
+        if constexpr (kWide) {
+            const int tpl = (S.nd + kWideLanes - 1) / kWideLanes;
+            status = tpl <= 2   ? o1w_stream<2>(S, sm, R, s_rows, out, lt)
+                     : tpl == 3 ? o1w_stream<3>(S, sm, R, s_rows, out, lt)
+                     : tpl == 4 ? o1w_stream<4>(S, sm, R, s_rows, out, lt)
+                                : o1w_stream<5>(S, sm, R, s_rows, out, lt);
+        } else {
+            status = o1s_stream(S, sm, R, out, lt);
+        }
         if (lane == 0) S.status = status;
         __syncwarp();
     }
 }
+static_assert((kDenseMax + kWideLanes - 1) / kWideLanes <= 5, "o1w_stream instantiations cover TPL <= 5");
 
 // ---------------------------------------------------------------------------
 // order-1, large alphabets: tables stay in global memory (L2), one dependent
@@ -1063,12 +1242,13 @@ __global__ void __launch_bounds__(32)
 // launchers
 // ---------------------------------------------------------------------------
 
-uint32_t dec_smem_bytes(int cls, int nd) {
+uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes) {
     switch (cls) {
         case kClsO0: return 16384 + kRingBytes;
-        case kClsO1Dense: return (uint32_t)align_up(dense_table_bytes(nd), 128) + kO1Warps * kRingBytes;
+        case kClsO1Dense: return (uint32_t)align_up(tbl_bytes, 128) + kO1Warps * kRingBytes;
         case kClsO1Global: return kRingBytes;
-        case kClsO1Small: return (uint32_t)align_up(dense_table_bytes(nd), 128) + kRingBytes;
+        case kClsO1Small:
+        case kClsO1Wide: return (uint32_t)align_up(tbl_bytes, 128) + kRingBytes;
         default: return 0;
     }
 }
@@ -1088,13 +1268,16 @@ static void ensure_dec_attrs() {
     }
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if (g_attr_done[dev]) return;
-    cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dec_smem_bytes(kClsO0, 0));
+    cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dec_smem_bytes(kClsO0, 0));
     cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)dec_smem_bytes(kClsO1Dense, kDenseMax));
+                         (int)dec_smem_bytes(kClsO1Dense, kDenseImageMax));
     cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)dec_smem_bytes(kClsO1Global, 0));
-    cudaFuncSetAttribute(dec_o1s_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)dec_smem_bytes(kClsO1Small, kSmallMaxNd));
+    cudaFuncSetAttribute(dec_o1w_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dec_smem_bytes(kClsO1Small, kDenseImageMax));
+    cudaFuncSetAttribute(dec_o1w_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)dec_smem_bytes(kClsO1Wide, kDenseImageMax));
     g_attr_done[dev] = true;
 }
 
@@ -1113,7 +1296,10 @@ int dec_blocks_per_sm(int cls, uint32_t smem_bytes) {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1g_kernel, 32, smem_bytes);
             break;
         case kClsO1Small:
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1s_kernel, 32, smem_bytes);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1w_kernel<false>, 32, smem_bytes);
+            break;
+        case kClsO1Wide:
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dec_o1w_kernel<true>, 32, smem_bytes);
             break;
         default:
             break;
@@ -1142,14 +1328,18 @@ void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint3
             break;
         case kClsO1Dense:
             dec_o1d_kernel<<<grid, kO1Threads, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                        smem_bytes - kO1Warps * kRingBytes, first_polls);
+                                                                smem_bytes - kO1Warps * kRingBytes, first_polls);
             break;
         case kClsO1Global:
             dec_o1g_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
             break;
         case kClsO1Small:
-            dec_o1s_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                      smem_bytes - kRingBytes, first_polls);
+            dec_o1w_kernel<false><<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
+                                                                smem_bytes - kRingBytes, first_polls);
+            break;
+        case kClsO1Wide:
+            dec_o1w_kernel<true><<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
+                                                               smem_bytes - kRingBytes, first_polls);
             break;
         default:
             break;

@@ -92,34 +92,47 @@ struct DecStream {
 };
 
 enum { kClsNone = 0, kClsO0 = 1, kClsO1Dense = 2, kClsO1Global = 3 };
-// Launch class of dense streams with |D| <= kSmallMaxNd (their tables are the
-// dense layout; one warp decodes a stream).
+// Launch classes of dense streams decoded by one warp each: |D| <=
+// kSmallMaxNd (every chain in its own lane) and wider alphabets (up to five
+// chains per lane). kClsO1Dense is then the four-warp decoder of the same
+// tables.
 constexpr int kClsO1Small = 4;
+constexpr int kClsO1Wide = 5;
 constexpr int kSmallMaxNd = 10;
 
 // Decode table arena per stream (bytes from tbl_off).
 //   order-0: 4096 x u32 packed ((freq - 1) << 20) | ((slot - cum) << 8) | sym.
-//   order-1 dense (|D| <= kDenseMax): D = present contexts and every symbol of
-//     their tables, in ascending byte order; DEAD = |D| marks "absent context".
-//     [0, chain_bytes)          chain table, u8: row d (stride 4100), slot -> dense
-//                               symbol (rows of absent contexts and DEAD: DEAD)
-//     [.., + fc_bytes)          u32 (freq << 12) | cum, row = context, col = symbol
+//   order-1 dense (|D| <= kDenseMax and an image of at most kDenseImageMax
+//     bytes): D = present contexts and every symbol of their tables, in
+//     ascending byte order; DEAD = |D| marks "absent context". The slot axis
+//     is cut at every position where some context's symbol changes (a
+//     boundary: a cum value of a present symbol); between two boundaries
+//     every context decodes every slot to the same symbol, so one column per
+//     boundary holds, for each context, the dense symbol of that slot range.
+//     [0, 8192)                 M: u16 per slot, the column of the slot in
+//                               16-byte units (column j * S / 16)
+//     [8192, + fc_bytes)        u32 (freq << 12) | cum, row = context, col = symbol
 //     [.., + 256)               dense index -> byte value
-//   order-1 global (more symbols): [256 B] raw context -> dense index (0xFF
-//     absent), then per present context t: 4096 x u16 (sym << 8) | dense(sym),
-//     then 256 x u32 (freq << 12) | cum.
+//     [col_off, + ncol * S)     columns, S = dense_col_stride(nd) bytes each:
+//                               byte d of column j = the dense symbol that
+//                               context d decodes in column j's slots (DEAD
+//                               for rows of absent contexts and for DEAD)
+//     Full-range quality tables (|D| ~ 31) have ~480 columns: ~28 KB against
+//     ~130 KB for a slot -> symbol table per context.
+//   order-1 global (more symbols, or more columns than the image holds):
+//     [256 B] raw context -> dense index (0xFF absent), then per present
+//     context t: 4096 x u16 (sym << 8) | dense(sym), then 256 x u32
+//     (freq << 12) | cum.
 constexpr int kDenseMax = 47;
-// Chain rows are 4100 bytes apart, not 4096: lanes that follow different
-// candidate contexts through the same slot then hit different banks.
-constexpr uint32_t kChainStride = 4100;
-__host__ __device__ inline uint32_t dense_chain_bytes(int nd) {
-    return (uint32_t)(((nd + 1) * kChainStride + 15) / 16 * 16);
-}
+constexpr uint32_t kDenseM = 8192;
+constexpr uint32_t kDenseImageMax = 160 * 1024;
+__host__ __device__ inline uint32_t dense_col_stride(int nd) { return (uint32_t)((nd + 1 + 15) / 16 * 16); }
 __host__ __device__ inline uint32_t dense_fc_bytes(int nd) {
     return (uint32_t)(((nd + 1) * (nd + 1) * 4 + 15) / 16 * 16);
 }
-__host__ __device__ inline uint32_t dense_table_bytes(int nd) {
-    return dense_chain_bytes(nd) + dense_fc_bytes(nd) + 256;
+__host__ __device__ inline uint32_t dense_col_off(int nd) { return kDenseM + dense_fc_bytes(nd) + 256; }
+__host__ __device__ inline uint32_t dense_table_bytes(int nd, uint32_t ncol) {
+    return dense_col_off(nd) + ncol * dense_col_stride(nd);
 }
 constexpr uint64_t kDecCtxMap = 0;
 constexpr uint64_t kDecO1Base = 256;
@@ -133,14 +146,13 @@ __host__ __device__ inline uint64_t dec_table_bytes(uint64_t src_len) {
     uint64_t b = 16384;
     if (k > 0) {
         const uint64_t g = kDecO1Base + k * kDecO1Ctx;
-        const uint64_t d = dense_table_bytes(kDenseMax);
         b = g > b ? g : b;
-        b = d > b ? d : b;
+        b = kDenseImageMax > b ? kDenseImageMax : b;
     }
     return b;
 }
 
-// Shared-memory layout of the decode kernels (one warp per CTA).
+// Shared-memory layout of the decode kernels.
 constexpr uint32_t kRingBytes = 2048;       // renorm-word ring, 4 x 512 B segments
 constexpr uint32_t kOutRows = 3 * kDenseMax + 1;
 
@@ -167,7 +179,7 @@ void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint
 void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
                     uint32_t first_polls, cudaStream_t s);
-uint32_t dec_smem_bytes(int cls, int nd);
+uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes);
 // CTAs of a decode class that fit on one SM with `smem_bytes` of dynamic
 // shared memory (registers and static shared memory included).
 int dec_blocks_per_sm(int cls, uint32_t smem_bytes);

@@ -80,7 +80,10 @@ MALFORMED = {1, 2, 3, 4, 5, 6, 7, 8}
 # Statuses a batch call reports per stream (the call itself succeeded):
 # the Malformed kinds and FQXV_RANS_E_TIMEOUT (a bounded device wait gave up).
 TIMEOUT = 21
-STREAM_STATUSES = MALFORMED | {TIMEOUT}
+# The extended format's own failure (include/fqxv_rans_x_gpu.h), no
+# reference counterpart.
+X_MALFORMED = 9
+STREAM_STATUSES = MALFORMED | {TIMEOUT, X_MALFORMED}
 
 
 def lib_path() -> str:

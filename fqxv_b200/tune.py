@@ -1,0 +1,195 @@
+"""Launch-shape sweep for one GPU model; writes the tuning table the library
+loads (fqxv_b200/tuning/<device>.json, see csrc/rans_tuning.cu).
+
+    python -m fqxv_b200.tune [--out PATH] [--reps 3]
+
+Every parameter is measured on batches of the stream types it governs
+(seeded synthetic data of the benchmark shapes), device-resident, with CUDA
+events, and set to the fastest value; the streams decoded or encoded are
+checked byte for byte against the input on every measurement. The
+reference's only run-time choice is its SIMD backend
+(crates/fqxv-rans/src/lib.rs:80-97); these are the GPU's counterparts:
+
+  o1_four_max_streams   below this many wide-alphabet order-1 streams in a
+                        launch group the four-warp decoder (one stream per
+                        SM, lower latency per stream) runs them, else the
+                        one-warp decoder (several streams per SM)
+  cta_cap_o0 / cta_cap_o1_small / cta_cap_o1_wide / cta_cap_o1_global
+                        CTAs per SM of each decode class (the occupancy
+                        API's figure is the upper bound)
+  dense_edge_small / dense_edge_large
+                        table-image sizes that cut dense order-1 streams
+                        into launch groups (a group's shared memory is its
+                        largest member's)
+  enc_run_ctas_per_sm   grid of the encode kernel, in CTAs per SM
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import workloads as W
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _batch(kind: str, nblocks: int, block: int, seed: int):
+    blobs = [W.GENERATORS[kind](block, seed + i) if kind != "ont" else W.ont_reads(block // 8000 + 2, seed + i)[:block]
+             for i in range(nblocks)]
+    data = np.concatenate(blobs)
+    lens = np.array([len(b) for b in blobs], dtype=np.uint64)
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint64)
+    return data, np.stack([offs, lens], 1)
+
+
+class Bench:
+    """Encode once (checked), then time decode / encode of one batch under a
+    parameter setting."""
+
+    def __init__(self, codec, data, spans, order):
+        import torch
+
+        self.c, self.data, self.spans, self.order = codec, data, spans, order
+        self.d_src = torch.from_numpy(data).cuda()
+        self.d_enc, self.es, _ = codec.encode_batch(self.d_src, spans, order)
+        self.d_dec = torch.empty(len(data), dtype=torch.uint8, device="cuda")
+        self.n = int(spans[:, 1].sum())
+
+    def _time(self, fn, reps):
+        import torch
+
+        fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s = torch.cuda.ExternalStream(self.c.stream_handle)
+            a.record(s)
+            fn()
+            b.record(s)
+            b.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return self.n / (best * 1e-3) / 1e9
+
+    def decode_gbs(self, reps):
+        import torch
+
+        def fn():
+            _, _, st = self.c.decode_batch(self.d_enc, self.es, self.spans, d_dst=self.d_dec)
+            assert (st == 0).all()
+        g = self._time(fn, reps)
+        assert torch.equal(self.d_dec, self.d_src), "decode differs from the input"
+        return g
+
+    def encode_gbs(self, reps):
+        enc_copy = self.d_enc.clone()
+
+        def fn():
+            self.c.encode_batch(self.d_src, self.spans, self.order, d_dst=self.d_enc)
+        g = self._time(fn, reps)
+        n = int(self.es[-1, 0] + self.es[-1, 1])
+        assert bool((self.d_enc[:n] == enc_copy[:n]).all()), "encode differs from the first encode"
+        return g
+
+
+def sweep(reps: int = 3) -> dict:
+    import torch
+
+    from .batch import Codec
+
+    c = Codec(0)
+    dev = torch.cuda.get_device_properties(0)
+    sms = dev.multi_processor_count
+    params, meas = {}, {}
+
+    def pick(name, values, gbs_of):
+        res = {}
+        for v in values:
+            c.set_param(name, v)
+            res[v] = gbs_of()
+        best = max(res, key=lambda v: res[v])
+        c.set_param(name, best)
+        params[name] = int(best)
+        meas["gbs_" + name] = {str(k): round(v, 3) for k, v in res.items()}
+        return best
+
+    # wide order-1 alphabets: four-warp against one-warp decoder by stream count
+    wide = {}
+    for count in (16, 64, sms, 2 * sms, 4 * sms):
+        data, spans = _batch("full", count, 256 << 10, 100)
+        b = Bench(c, data, spans, 1)
+        row = {}
+        for name, v in (("four", 1 << 30), ("wide", 0)):
+            c.set_param("o1_four_max_streams", v)
+            row[name] = b.decode_gbs(reps)
+        wide[count] = row
+        del b
+    crossover = next((k for k in sorted(wide) if wide[k]["wide"] >= wide[k]["four"]), 1 << 30)
+    params["o1_four_max_streams"] = int(crossover)
+    c.set_param("o1_four_max_streams", crossover)
+    meas["gbs_o1_wide_vs_four_by_streams"] = {str(k): {n: round(g, 3) for n, g in v.items()} for k, v in wide.items()}
+
+    caps = (1, 2, 4, 8, 16, 32)
+    b = Bench(c, *_batch("binned", 1024, 256 << 10, 200), 0)
+    pick("cta_cap_o0", caps, lambda: b.decode_gbs(reps))
+    del b
+    b = Bench(c, *_batch("binned", 1024, 256 << 10, 300), 1)
+    pick("cta_cap_o1_small", caps, lambda: b.decode_gbs(reps))
+    del b
+    b = Bench(c, *_batch("full", 1024, 256 << 10, 400), 1)
+    pick("cta_cap_o1_wide", caps, lambda: b.decode_gbs(reps))
+    del b
+    # dense group edges on a mix of wide-alphabet types (name tokens, full-range, long-read quality)
+    parts = [_batch(k, 256, 256 << 10, 500 + i) for i, k in enumerate(("names", "full", "ont"))]
+    data = np.concatenate([p[0] for p in parts])
+    spans = np.concatenate([p[1] for p in parts]).copy()
+    base = 0
+    for p, q in zip(parts, range(3)):
+        spans[q * 256:(q + 1) * 256, 0] += base
+        base += len(p[0])
+    b = Bench(c, data, spans, 1)
+    res = {}
+    for lo, hi in ((24 << 10, 48 << 10), (32 << 10, 64 << 10), (40 << 10, 80 << 10), (48 << 10, 96 << 10),
+                   (64 << 10, 128 << 10)):
+        c.set_param("dense_edge_small", lo)
+        c.set_param("dense_edge_large", hi)
+        res[(lo, hi)] = b.decode_gbs(reps)
+    lo, hi = max(res, key=lambda k: res[k])
+    params["dense_edge_small"], params["dense_edge_large"] = int(lo), int(hi)
+    c.set_param("dense_edge_small", lo)
+    c.set_param("dense_edge_large", hi)
+    meas["gbs_dense_edges"] = {"%d/%d" % k: round(v, 3) for k, v in res.items()}
+    del b
+    # encode grid on a mixed batch of both orders (config 2's stream types)
+    data, spans, _ = W.config2(nblocks=512, hi=1 << 20, seed=600)
+    b = Bench(c, data, spans, 2)
+    pick("enc_run_ctas_per_sm", (4, 8, 16, 32), lambda: b.encode_gbs(reps))
+    del b
+    c.close()
+    return {"device": dev.name, "sm_count": sms, "params": params, "measurements": meas,
+            "when": time.strftime("%Y-%m-%d %H:%M:%S")}
+
+
+def main():
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args()
+    res = sweep(args.reps)
+    stem = "".join(ch.lower() if ch.isalnum() else "_" for ch in torch.cuda.get_device_properties(0).name)
+    out = args.out or os.path.join(HERE, "tuning", stem + ".json")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    with open(out, "w") as f:
+        json.dump(res, f, indent=1)
+    print(json.dumps(res["params"]))
+
+
+if __name__ == "__main__":
+    main()

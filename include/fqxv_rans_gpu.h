@@ -49,6 +49,9 @@ typedef enum fqxv_rans_status {
      * reference's SIMD backends say this; this decoder follows scalar.rs and
      * reports FQXV_RANS_E_TRUNCATED instead. Kept for numbering parity. */
     FQXV_RANS_E_TRUNCATED_RENORM = 8,
+    /* Extended format only (fqxv_rans_x_gpu.h; no reference counterpart):
+     * its transform data does not fit together. */
+    FQXV_RANS_E_X_MALFORMED = 9,
     /* API errors (no reference counterpart). */
     FQXV_RANS_E_INVALID_ARG = 16,
     FQXV_RANS_E_DST_TOO_SMALL = 17,
@@ -231,6 +234,22 @@ int fqxv_rans_server_stats(fqxv_rans_server *server, uint64_t *completed, uint64
  * code while doing so, so make it before any stream capture. */
 int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int order, uint8_t *d_dst, size_t dst_cap,
                              size_t *out_len, void *stream);
+
+/* ---- launch shapes -------------------------------------------------------
+ * No reference counterpart beyond Backend::detect (lib.rs:80-97). Every
+ * context has integer launch-shape parameters (decoder choice for wide
+ * order-1 alphabets by stream count, CTAs per SM of each decode class,
+ * dense-table group edges, encode grid); they start from the tuning table of
+ * the device when one is found (FQXV_RANS_TUNING, else tuning/<device>.json
+ * beside the package directory of the library), else from the built-in
+ * rules. Names: o1_four_max_streams, cta_cap_o0, cta_cap_o1_small,
+ * cta_cap_o1_wide, cta_cap_o1_four, cta_cap_o1_global, dense_edge_small,
+ * dense_edge_large, enc_run_ctas_per_sm. Unknown names and out-of-range
+ * values: FQXV_RANS_E_INVALID_ARG. Output bytes never depend on them. */
+int fqxv_rans_ctx_set_param(fqxv_rans_ctx *ctx, const char *name, int64_t value);
+int fqxv_rans_ctx_get_param(fqxv_rans_ctx *ctx, const char *name, int64_t *value);
+/* Path of the tuning table the context applied ("" when none). */
+const char *fqxv_rans_ctx_tuning_source(fqxv_rans_ctx *ctx);
 
 /* ---- per-stage device timing -------------------------------------------
  * When enabled, every kernel launch of a context is bracketed by CUDA events

@@ -28,6 +28,7 @@ MESSAGES = {
     6: "rANS output length too large to allocate",
     7: "rANS output length exceeds caller bound",
     8: "truncated renorm stream",
+    9: "malformed extended stream",
     16: "invalid argument",
     17: "destination buffer too small",
     32: "truncated fqxv stream",
@@ -306,3 +307,80 @@ def crc32c_batch(src: np.ndarray, offs, lens, nthreads: int = 0) -> np.ndarray:
     lib().orc_crc32c_batch(_ptr(src, ctypes.c_uint8), _ptr(offs, ctypes.c_uint64), _ptr(lens, ctypes.c_uint64),
                            len(offs), _ptr(out, ctypes.c_uint32), nthreads)
     return out[:len(offs)]
+
+# --- extended stream format (rans_x.c): PARITY UNPINNED, test infrastructure
+
+
+X_ORDER1, X_N4, X_STRIPE, X_RLE, X_PACK, X_CAT = 0x01, 0x02, 0x04, 0x08, 0x10, 0x20
+X_MALFORMED = 9
+
+
+def _x_lib():
+    L = lib()
+    if not getattr(L, "_x_ready", False):
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        sz = ctypes.c_size_t
+        szp = ctypes.POINTER(ctypes.c_size_t)
+        L.orc_x_encode_bound.restype = sz
+        L.orc_x_encode_bound.argtypes = [sz, ctypes.c_int]
+        L.orc_x_best_bound.restype = sz
+        L.orc_x_best_bound.argtypes = [sz]
+        L.orc_x_encode.argtypes = [u8p, sz, ctypes.c_int, u8p, sz, szp]
+        L.orc_x_decode.argtypes = [u8p, sz, u8p, sz, szp]
+        L.orc_x_encode_best.argtypes = [u8p, sz, u8p, sz, szp, ctypes.POINTER(ctypes.c_int)]
+        L.orc_core_encode.argtypes = [u8p, sz, ctypes.c_int, ctypes.c_int, u8p, szp]
+        L.orc_core_bound.restype = sz
+        L.orc_core_bound.argtypes = [sz, ctypes.c_int, ctypes.c_int]
+        L._x_ready = True
+    return L
+
+
+def x_encode(data, flags: int) -> bytes:
+    """The extended stream of `data` with transform flags `flags`."""
+    L = _x_lib()
+    a, p = _buf(data)
+    cap = L.orc_x_encode_bound(a.size, flags)
+    out = np.empty(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    st = L.orc_x_encode(p, a.size, flags, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), cap, ctypes.byref(n))
+    if st:
+        raise OracleError(st)
+    return out[:n.value].tobytes()
+
+
+def x_encode_best(data) -> tuple[bytes, int]:
+    """(stream, candidate index) of the selection over reference and
+    extended candidates."""
+    L = _x_lib()
+    a, p = _buf(data)
+    cap = L.orc_x_best_bound(a.size)
+    out = np.empty(cap, dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    c = ctypes.c_int(0)
+    st = L.orc_x_encode_best(p, a.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), cap, ctypes.byref(n),
+                             ctypes.byref(c))
+    if st:
+        raise OracleError(st)
+    return out[:n.value].tobytes(), c.value
+
+
+def x_decode(stream, cap: int | None = None) -> bytes:
+    """Decode an extended (or reference) stream; raises OracleError."""
+    L = _x_lib()
+    a, p = _buf(stream)
+    if cap is None:
+        cap = int.from_bytes(bytes(a[1:9]), "little") if a.size >= 9 else 0
+    out = np.empty(max(cap, 1), dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    st = L.orc_x_decode(p, a.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), cap, ctypes.byref(n))
+    if st:
+        raise OracleError(st)
+    return out[:n.value].tobytes()
+
+
+def x_decode_status(stream, cap: int) -> int:
+    L = _x_lib()
+    a, p = _buf(stream)
+    out = np.empty(max(cap, 1), dtype=np.uint8)
+    n = ctypes.c_size_t(0)
+    return L.orc_x_decode(p, a.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), cap, ctypes.byref(n))

@@ -38,6 +38,7 @@ enum {
     ORC_E_ALLOC = 6,             /* "rANS output length too large to allocate" model.rs:202 */
     ORC_E_BOUND = 7,             /* "rANS output length exceeds caller bound" lib.rs:228 */
     ORC_E_TRUNCATED_RENORM = 8,  /* "truncated renorm stream"           avx2.rs:207 */
+    ORC_E_X_MALFORMED = 9,       /* extended format only (rans_x.c): inconsistent transform data */
     ORC_E_INVALID_ARG = 16,
     ORC_E_DST_TOO_SMALL = 17,
     /* container frames (crates/fqxv/src/lib.rs:167-178, block.rs:1209-1254) */
@@ -118,6 +119,33 @@ int orc_encode_batch(const uint8_t *src, const uint64_t *src_off, const uint64_t
 int orc_decode_batch(const uint8_t *src, const uint64_t *src_off, const uint64_t *src_len,
                      size_t nblocks, uint8_t *dst, const uint64_t *dst_off,
                      const uint64_t *dst_cap, uint64_t *out_len, int32_t *status, int nthreads);
+
+/* ---- Extended stream format (rans_x.c): PARITY UNPINNED -------------------
+ * A new format tag (first byte 0x80 | flags) with no counterpart in the
+ * reference: 4-way interleaved cores and the STRIPE / RLE / PACK / CAT
+ * transforms. Layout in rans_x.c. */
+enum {
+    ORC_X_ORDER1 = 0x01,
+    ORC_X_N4 = 0x02,
+    ORC_X_STRIPE = 0x04,
+    ORC_X_RLE = 0x08,
+    ORC_X_PACK = 0x10,
+    ORC_X_CAT = 0x20,
+    ORC_X_ALL = 0x3f
+};
+/* Cores: nstates 32 is the reference stream (orc_encode); 4 writes tag
+ * 2 | order with four states. Decode takes either. */
+size_t orc_core_bound(size_t n, int order, int nstates);
+int orc_core_encode(const uint8_t *src, size_t n, int order, int nstates, uint8_t *dst, size_t *out_len);
+int orc_core_decode(const uint8_t *src, size_t len, uint8_t *dst, size_t cap, size_t *out_len);
+size_t orc_x_encode_bound(size_t n, int flags);
+int orc_x_encode(const uint8_t *src, size_t n, int flags, uint8_t *dst, size_t dst_cap, size_t *out_len);
+/* Decodes an extended stream, or a reference stream (first byte < 0x80). */
+int orc_x_decode(const uint8_t *src, size_t len, uint8_t *dst, size_t dst_cap, size_t *out_len);
+/* The selection over reference and extended candidates (rans_x.c); *cand
+ * receives the winning candidate's index. */
+size_t orc_x_best_bound(size_t n);
+int orc_x_encode_best(const uint8_t *src, size_t n, uint8_t *dst, size_t dst_cap, size_t *out_len, int *cand);
 
 /* ---- CRC-32C and block frames (frame_oracle.c) ------------------------
  * crates/fqxv/src/crc.rs and crates/fqxv/src/container/block.rs. */
