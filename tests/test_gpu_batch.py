@@ -242,3 +242,38 @@ def test_host_batches_in_chunks_match_single_pass(codec, orc):
         assert st[i] == 0 and lens[i] == spans[i, 1]
         o, l = int(spans[i, 0]), int(spans[i, 1])
         assert np.array_equal(h_dec[o:o + l], data[o:o + l]), i
+
+
+def test_launch_shapes_change_no_byte(codec):
+    """Launch-shape parameters (fqxv_rans_ctx_set_param) move work between
+    decoders and change grids; the streams and the decoded bytes stay the
+    same."""
+    import torch
+
+    data, spans, _ = W.config2(nblocks=40, lo=1000, hi=400_000, seed=77)
+    d_src = _dev(data)
+    ref_out, ref_spans, _ = codec.encode_batch(d_src, spans, 2)
+    ref = ref_out[:int(ref_spans[-1, 0] + ref_spans[-1, 1])].cpu().numpy()
+    settings = [
+        {"o1_four_max_streams": 0, "cta_cap_o1_wide": 1, "enc_run_ctas_per_sm": 4},
+        {"o1_four_max_streams": 1 << 30, "cta_cap_o1_four": 1, "dense_edge_small": 0, "dense_edge_large": 0},
+        {"cta_cap_o0": 1, "cta_cap_o1_small": 2, "dense_edge_small": 160 << 10, "dense_edge_large": 160 << 10},
+    ]
+    defaults = {k: codec.get_param(k) for s in settings for k in s}
+    try:
+        for st in settings:
+            for k, v in st.items():
+                codec.set_param(k, v)
+            out, osp, _ = codec.encode_batch(d_src, spans, 2)
+            assert np.array_equal(osp, ref_spans)
+            assert np.array_equal(out[:len(ref)].cpu().numpy(), ref)
+            d_dec, lens, stt = codec.decode_batch(out, osp, spans)
+            assert (stt == 0).all()
+            assert torch.equal(d_dec[:len(data)], d_src[:len(data)])
+    finally:
+        for k, v in defaults.items():
+            codec.set_param(k, v)
+    with pytest.raises(Exception):
+        codec.set_param("no_such_parameter", 1)
+    with pytest.raises(Exception):
+        codec.set_param("cta_cap_o0", 0)
