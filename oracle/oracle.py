@@ -384,3 +384,27 @@ def x_decode_status(stream, cap: int) -> int:
     out = np.empty(max(cap, 1), dtype=np.uint8)
     n = ctypes.c_size_t(0)
     return L.orc_x_decode(p, a.size, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), cap, ctypes.byref(n))
+
+
+def x_encode_batch(src: np.ndarray, offs, lens, flags: int, nthreads: int = 0):
+    """Extended-format encode of every block on all host cores (flags 0x40:
+    the selection). Returns (arena, offsets, lengths, choices)."""
+    L = _x_lib()
+    nb = len(offs)
+    offs = np.ascontiguousarray(offs, dtype=np.uint64)
+    lens = np.ascontiguousarray(lens, dtype=np.uint64)
+    caps = np.array([L.orc_x_best_bound(int(n)) for n in lens], dtype=np.uint64)
+    doff = np.zeros(nb, dtype=np.uint64)
+    if nb:
+        doff[1:] = np.cumsum(caps)[:-1]
+    dst = np.empty(max(int(caps.sum()), 1), dtype=np.uint8)
+    ol = np.zeros(nb, dtype=np.uint64)
+    st = np.zeros(nb, dtype=np.int32)
+    ch = np.zeros(nb, dtype=np.int32)
+    L.orc_x_batch.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_size_t, ctypes.c_int, ctypes.c_int] + \
+        [ctypes.c_void_p] * 6 + [ctypes.c_int]
+    rc = L.orc_x_batch(src.ctypes.data, offs.ctypes.data, lens.ctypes.data, nb, flags, 0, dst.ctypes.data,
+                       doff.ctypes.data, caps.ctypes.data, ol.ctypes.data, st.ctypes.data, ch.ctypes.data, nthreads)
+    if rc:
+        raise OracleError(rc)
+    return dst, doff, ol, ch

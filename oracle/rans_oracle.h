@@ -146,6 +146,11 @@ int orc_x_decode(const uint8_t *src, size_t len, uint8_t *dst, size_t dst_cap, s
  * receives the winning candidate's index. */
 size_t orc_x_best_bound(size_t n);
 int orc_x_encode_best(const uint8_t *src, size_t n, uint8_t *dst, size_t dst_cap, size_t *out_len, int *cand);
+/* Blocks in parallel on all host cores: encode with `flags` (0x40: the
+ * selection; choice[i] gets the candidate) or, with decode != 0, decode. */
+int orc_x_batch(const uint8_t *src, const uint64_t *src_off, const uint64_t *src_len, size_t nblocks, int flags,
+                int decode, uint8_t *dst, const uint64_t *dst_off, const uint64_t *dst_cap, uint64_t *out_len,
+                int32_t *status, int32_t *choice, int nthreads);
 
 /* ---- CRC-32C and block frames (frame_oracle.c) ------------------------
  * crates/fqxv/src/crc.rs and crates/fqxv/src/container/block.rs. */

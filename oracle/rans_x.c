@@ -634,3 +634,62 @@ int orc_x_encode_best(const uint8_t *src, size_t n, uint8_t *dst, size_t dst_cap
     if (dst_cap < orc_x_best_bound(n)) return ORC_E_DST_TOO_SMALL;
     return best_of(src, n, 0, dst, out_len, cand);
 }
+
+/* ---- block-parallel batch over all host cores (the CPU check of the GPU's
+ * batches): flags a transform combination, or 0x40 for the selection. ---- */
+#include <pthread.h>
+#include <stdatomic.h>
+#include <unistd.h>
+
+typedef struct {
+    const uint8_t *src;
+    const uint64_t *src_off, *src_len;
+    size_t nblocks;
+    int flags, decode;
+    uint8_t *dst;
+    const uint64_t *dst_off, *dst_cap;
+    uint64_t *out_len;
+    int32_t *status, *choice;
+    atomic_size_t next;
+} x_job;
+
+static void *x_worker(void *arg) {
+    x_job *J = (x_job *)arg;
+    for (;;) {
+        const size_t i = atomic_fetch_add(&J->next, 1);
+        if (i >= J->nblocks) break;
+        const uint8_t *s = J->src + J->src_off[i];
+        uint8_t *d = J->dst + J->dst_off[i];
+        size_t ol = 0;
+        int st, c = J->flags;
+        if (J->decode)
+            st = orc_x_decode(s, J->src_len[i], d, J->dst_cap[i], &ol);
+        else if (J->flags == 0x40)
+            st = orc_x_encode_best(s, J->src_len[i], d, J->dst_cap[i], &ol, &c);
+        else
+            st = orc_x_encode(s, J->src_len[i], J->flags, d, J->dst_cap[i], &ol);
+        J->out_len[i] = ol;
+        J->status[i] = st;
+        if (J->choice) J->choice[i] = c;
+    }
+    return NULL;
+}
+
+int orc_x_batch(const uint8_t *src, const uint64_t *src_off, const uint64_t *src_len, size_t nblocks, int flags,
+                int decode, uint8_t *dst, const uint64_t *dst_off, const uint64_t *dst_cap, uint64_t *out_len,
+                int32_t *status, int32_t *choice, int nthreads) {
+    x_job J = {src, src_off, src_len, nblocks, flags, decode, dst, dst_off, dst_cap, out_len, status, choice};
+    atomic_init(&J.next, 0);
+    if (nthreads <= 0) nthreads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (nthreads < 1) nthreads = 1;
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)nthreads);
+    int started = 0;
+    for (int t = 1; t < nthreads && th; t++)
+        if (pthread_create(&th[started], NULL, x_worker, &J) == 0) started++;
+    x_worker(&J);
+    for (int t = 0; t < started; t++) pthread_join(th[t], NULL);
+    free(th);
+    for (size_t i = 0; i < nblocks; i++)
+        if (status[i]) return status[i];
+    return ORC_OK;
+}
