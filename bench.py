@@ -21,6 +21,10 @@ Workloads (seeded synthetic data of the benchmark shapes):
            full-range order-1: peak batched throughput of one order
   cpu_single (with --impl reference)  the CPU coder on one thread, 8 MiB of
            quality_like data, per path (the reference's own benchmark shape)
+  xconfig0 / xconfig2  the extended format (a new format tag, no reference
+           counterpart): config 0 as named (4-way, order-0) and config 2 with the
+           selection over reference and extended candidates, every stream
+           checked against its CPU definition
   names    read-name tokenizer (crates/fqxv-tokenizer): 256 blocks x 4000
            Illumina-style names, encode then decode through the C ABI
   crc      CRC-32C of 4096 payloads 4 KiB - 4 MiB (crates/fqxv/src/crc.rs)
@@ -512,6 +516,114 @@ def run_names_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+X_METRIC = "extended format (4-way cores, STRIPE/RLE/PACK/CAT) enc/dec GB/s, identical to its CPU definition"
+
+
+def run_xformat(args, rank: int, world: int, local: int, dist) -> None:
+    """xconfig0: config 0 as named -- one 1 MiB block of binned quality,
+    order-0, 4-way interleave (flags 0x02). xconfig2: config 2's 4096 mixed
+    blocks, the selection over reference and extended candidates (0x40).
+    A step is the GPU encode of every block then the decode of its streams;
+    every stream is checked against the CPU definition (oracle/rans_x.c,
+    parity unpinned against the reference, which has no such format)."""
+    import torch
+
+    from fqxv_b200.batch import Codec
+    from oracle import oracle
+
+    if args.workload == "xconfig0":
+        data, spans = W.config0(seed=args.seed + rank)
+        flags, desc = 0x02, "1 x 1 MiB binned quality, order-0, 4-way interleave"
+    else:
+        data, spans, _ = W.config2(nblocks=args.blocks or 4096, seed=args.seed + rank,
+                                   workers=min(32, os.cpu_count() or 1))
+        flags, desc = 0x40, "%d mixed blocks 4 KiB-4 MiB, smallest of reference and extended candidates" % len(spans)
+    n_bytes = int(spans[:, 1].sum())
+    codec = Codec(local)
+    cs = torch.cuda.ExternalStream(codec.stream_handle)
+    d_src = torch.from_numpy(data).to("cuda")
+    d_dec = torch.empty(max(n_bytes, 1), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def step():
+        d_enc, es, ch = codec.x_encode_batch(d_src, spans, flags)
+        _, lens, st = codec.x_decode_batch(d_enc, es, spans, d_dst=d_dec)
+        return d_enc, es, ch, st
+
+    for _ in range(args.warmup):
+        d_enc, es, ch, st = step()
+    torch.cuda.synchronize()
+    assert (st == 0).all() and torch.equal(d_dec[:n_bytes], d_src[:n_bytes]), "round trip mismatch"
+    identity = None
+    if rank == 0 and not args.no_identity:
+        ref, roff, rlen, rch = oracle.x_encode_batch(data, spans[:, 0], spans[:, 1], flags)
+        got = d_enc[:int(es[-1, 0] + es[-1, 1])].cpu().numpy()
+        same = sum(1 for i in range(len(spans)) if int(es[i, 1]) == int(rlen[i]) and np.array_equal(
+            got[int(es[i, 0]):int(es[i, 0] + es[i, 1])], ref[int(roff[i]):int(roff[i] + rlen[i])]))
+        kinds = {int(k): int((rch == k).sum()) for k in np.unique(rch)}
+        identity = {"blocks": "%d/%d" % (same, len(spans)), "choices_equal": bool((ch == rch).all()),
+                    "choice_counts": kinds}
+    codec.stage_stats(reset=True)
+    codec.set_profiling(True)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    total_ms = 0.0
+    comp = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cs)
+        d_enc, es, ch, st = step()
+        b.record(cs)
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+        comp = int(es[:, 1].sum())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    codec.set_profiling(False)
+    stages = codec.stage_stats(reset=True)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t[0])
+    value = world * n_bytes * args.steps / (total_ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        nthreads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < 5.0 and reps < 5:
+            oracle.x_encode_batch(data, spans[:, 0], spans[:, 1], flags, nthreads)
+            reps += 1
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(n_bytes * reps / dt / 1e9, 4), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": "%d encode passes of the whole workload by the CPU definition (oracle/rans_x.c) on %d "
+                         "host threads" % (reps, nthreads)}
+    if rank == 0:
+        line = {
+            "metric": X_METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": desc, "blocks": int(len(spans)), "bytes_per_gpu": n_bytes,
+                       "compressed_bytes_per_gpu": comp, "flags": flags,
+                       "l2": "flushed (256 MiB write) before every timed step",
+                       "parity": "against the CPU definition; unpinned against the reference (no such format)"},
+            "identity": identity, "cpu_baseline": cpu,
+            "gpu_launches": int(sum(v["launches"] for v in stages.values())),
+            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "wall_ms": round(v["wall_ms"], 4)}
+                       for k, v in stages.items() if v["launches"]},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    codec.close()
+
+
 def peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -701,6 +813,11 @@ def run_reference(args, rank: int) -> None:
         return
     if args.workload == "names":
         run_names_reference(args)
+        return
+    if args.workload.startswith("x"):
+        print(json.dumps({"impl": "reference", "unavailable": "fqxv-rans writes only its 32-way untagged format; the "
+                          "extended format has no reference implementation (crates/fqxv-rans/src/model.rs:19, "
+                          "scalar.rs:8-20)"}), flush=True)
         return
     data, spans, order, desc, extra = build_workload(args.workload, args.seed, args.blocks)
     nthreads = os.cpu_count() or 1
@@ -952,7 +1069,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="config2",
                     choices=["config1", "config0", "config2", "config3", "config4", "batch0", "batch1", "batch1f",
-                             "cpu_single", "crc", "frame", "names"])
+                             "cpu_single", "crc", "frame", "names", "xconfig0", "xconfig2"])
     ap.add_argument("--requests", type=int, default=48, help="config4: requests per load level")
     ap.add_argument("--workers", type=int, default=8, help="config4: server workers (streams)")
     ap.add_argument("--loads", type=float, nargs="+", default=[0.25, 0.5, 0.75, 1.0])
@@ -995,8 +1112,9 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    if args.workload in FRAME_METRICS or args.workload == "names":
-        (run_names if args.workload == "names" else run_frames)(args, rank, world, local, dist)
+    if args.workload in FRAME_METRICS or args.workload in ("names", "xconfig0", "xconfig2"):
+        fn = run_names if args.workload == "names" else run_xformat if args.workload.startswith("x") else run_frames
+        fn(args, rank, world, local, dist)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

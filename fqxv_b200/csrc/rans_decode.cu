@@ -247,24 +247,28 @@ __global__ void __launch_bounds__(kParseThreads)
                         s_ncol = (int)tot;
                     }
                     __syncthreads();
-                    dense = dense_table_bytes(nd, (uint32_t)s_ncol) <= kDenseImageMax;
+                    dense = dense_build_bytes(nd, (uint32_t)s_ncol) <= kDenseImageMax;
                 }
                 if (dense) {
                     const uint32_t ncol = (uint32_t)s_ncol;
                     const int dead = nd;
                     const int stride = nd + 1;
                     const uint32_t cs = dense_col_stride(nd);
+                    const bool packed = dense_packed(nd);
                     uint16_t *M = reinterpret_cast<uint16_t *>(T);
                     uint32_t *FC = reinterpret_cast<uint32_t *>(T + kDenseM);
                     uint8_t *DS = T + kDenseM + dense_fc_bytes(nd);
-                    uint8_t *COL = T + dense_col_off(nd);
+                    // byte columns: the image itself, or (packed form) scratch
+                    // after it from which the u64 columns are packed
+                    uint8_t *COL = T + (packed ? dense_table_bytes(nd, ncol) : dense_col_off(nd));
                     // Every column entry starts DEAD (rows of contexts without
                     // a table, the DEAD row, padding); FC starts zeroed.
                     const uint32_t deadw = 0x01010101u * (uint32_t)dead;
                     for (uint32_t i = tid; i < ncol * cs / 4; i += blockDim.x)
                         reinterpret_cast<uint32_t *>(COL)[i] = deadw;
                     for (int i = tid; i < stride * stride; i += blockDim.x) FC[i] = 0;
-                    for (int i = tid; i < (int)kTotFreq; i += blockDim.x) M[i] = (uint16_t)(s_col[i] * (cs >> 4));
+                    for (int i = tid; i < (int)kTotFreq; i += blockDim.x)
+                        M[i] = (uint16_t)(packed ? s_col[i] : s_col[i] * (cs >> 4));
                     if (tid < 256 && dmap[tid] != 0xff) DS[dmap[tid]] = (uint8_t)tid;
                     __syncthreads();
                     // One warp per present context: its FC row, and its row
@@ -294,6 +298,16 @@ __global__ void __launch_bounds__(kParseThreads)
                         }
                     }
                     __syncthreads();
+                    if (packed) {
+                        // 16 entries of a 16-byte column -> 16 nibbles
+                        uint64_t *PK = reinterpret_cast<uint64_t *>(T + dense_col_off(nd));
+                        for (uint32_t j = tid; j < ncol; j += blockDim.x) {
+                            uint64_t v = 0;
+                            for (int d = 0; d < 16; d++) v |= (uint64_t)(COL[j * cs + d] & 15u) << (4 * d);
+                            PK[j] = v;
+                        }
+                        __syncthreads();
+                    }
                     if (tid == 0) {
                         S.cls = kClsO1Dense;
                         S.nd = nd;
@@ -670,10 +684,27 @@ __device__ __forceinline__ void named_bar(int id) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kO1Threads) : "memory");
 }
 
+// A slot's column, as the chains of a round need it: byte columns give the
+// column's byte offset from the column base (a chain step is then one byte
+// load); packed columns give the column itself, 16 four-bit entries in a
+// u64 (a chain step is then a shift of a register).
+struct ByteCols {
+    const uint16_t *M;
+    using T = uint32_t;
+    __device__ __forceinline__ T operator()(uint32_t slot) const { return (uint32_t)M[slot] << 4; }
+};
+struct PackedCols {
+    const uint16_t *M;
+    const uint64_t *PK;
+    using T = uint64_t;
+    __device__ __forceinline__ T operator()(uint32_t slot) const { return PK[M[slot]]; }
+};
+
 // The rounds of one order-1 dense stream (scalar.rs:202-215), shared by the
-// 4-warp and the 1-warp decoders: `resolve(slot, cb, d, ctx)` runs one
-// round's context chain and gives this lane's symbol and context; `store`
-// says whether this warp writes the output.
+// 4-warp and the 1-warp decoders: `resolve(slot, col, d, ctx)` runs one
+// round's context chain from every lane's column (`Col`: byte or packed
+// columns) and gives this lane's symbol and context; `store` says whether
+// this warp writes the output.
 //
 // Rounds that cannot run out of words (and are not the first or the partial
 // last round) take a branch-free fast path: the ring advances by predication,
@@ -682,18 +713,18 @@ __device__ __forceinline__ void named_bar(int id) {
 // come earlier inside those rounds. Other rounds take the careful path with
 // every check of scalar.rs:202-215 in order.
 //
-// `resolve` gets the lane's slot and the byte offset of its column (M[slot]
-// in 16-byte units, times 16). In fast rounds the next round's column is
-// found while this round renormalises: a lane that takes a word gets its
+// `resolve` gets the lane's slot and its column. In fast rounds the next
+// round's column is found while this round renormalises: a lane that takes a word gets its
 // column with it (the column of every candidate word is looked up when the
 // window is read, and shuffled along with the word); a lane that takes none
 // looks up the column of its new value while the vote runs. So the M lookup
 // is off the chain from one round to the next.
-template <class Resolve>
+template <class Col, class Resolve>
 __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__restrict__ out, uint32_t lt,
-                                         const uint16_t *__restrict__ M, const uint32_t *__restrict__ FC,
+                                         const Col &C, const uint32_t *__restrict__ FC,
                                          const uint8_t *__restrict__ DS, uint32_t stride, uint32_t dead, bool store,
                                          uint32_t x, Resolve &&resolve) {
+    using CT = typename Col::T;
     const int lane = threadIdx.x & 31;
     const uint64_t n = S.n;
     const uint64_t navail = S.words_len / 2;
@@ -713,7 +744,7 @@ __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__r
             const bool active = i < n;
             const uint32_t slot = x & (kTotFreq - 1);
             uint32_t d, ctx;
-            resolve(slot, (uint32_t)M[slot] << 4, d, ctx);
+            resolve(slot, C(slot), d, ctx);
             const uint32_t deadmask = __ballot_sync(0xffffffffu, active && d == dead);
             const int absent_at = deadmask ? __ffs(deadmask) - 1 : 32;
             const bool valid = active && lane < absent_at;
@@ -741,7 +772,7 @@ __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__r
         uint32_t adv_at = (uint32_t)((512u * (uint32_t)(R.next_seg - 3) - R.lead + 1u) / 2u);
         uint32_t sawdead = 0;
         uint8_t *op = out + r * 32 + lane;
-        uint32_t cb = (uint32_t)M[x & (kTotFreq - 1)] << 4;
+        CT cb = C(x & (kTotFreq - 1));
         for (int64_t c = 0; c < cnt; c++) {
             // predicated one-segment ring advance (a round moves <= 64 bytes)
             const bool adv = w32 - (uint32_t)wp >= adv_at - (uint32_t)wp;
@@ -753,19 +784,19 @@ __device__ __forceinline__ int o1_rounds(DecStream &S, WordRing &R, uint8_t *__r
             }
             __syncwarp();
             const uint32_t cand = R.word(w32 + lane);
-            const uint32_t cbc = (uint32_t)M[cand & (kTotFreq - 1)] << 4;
+            const CT cbc = C(cand & (kTotFreq - 1));
             const uint32_t slot = x & (kTotFreq - 1);
             uint32_t d, ctx;
             resolve(slot, cb, d, ctx);
             sawdead |= d == dead;
             const uint32_t fc = FC[ctx * stride + d];
             const uint32_t v = (fc >> kScaleBits) * (x >> kScaleBits) + slot - (fc & (kTotFreq - 1));
-            const uint32_t cbv = (uint32_t)M[v & (kTotFreq - 1)] << 4;
+            const CT cbv = C(v & (kTotFreq - 1));
             const bool need = v < kRansL;
             const uint32_t mask = __ballot_sync(0xffffffffu, need);
             const uint32_t srcl = __popc(mask & lt) & 31;
             const uint32_t w = __shfl_sync(0xffffffffu, cand, srcl);
-            const uint32_t cbw = __shfl_sync(0xffffffffu, cbc, srcl);
+            const CT cbw = __shfl_sync(0xffffffffu, cbc, srcl);
             if (store) *op = DS[d];
             op += 32;
             x = need ? (v << 16) | w : v;
@@ -889,7 +920,7 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         buf ^= 1u;
     };
 
-    return o1_rounds(S, R, out, lt, I.M, I.FC, I.DS, I.stride, dead, warp == 0, x, resolve);
+    return o1_rounds(S, R, out, lt, ByteCols{I.M}, I.FC, I.DS, I.stride, dead, warp == 0, x, resolve);
 }
 
 __global__ void __launch_bounds__(kO1Threads, 1)
@@ -942,13 +973,16 @@ __global__ void __launch_bounds__(kO1Threads, 1)
 // order-1, one warp per stream
 // ---------------------------------------------------------------------------
 
-// Small alphabets (|D| <= kSmallMaxNd): every chain fits in one warp: lane 0
-// runs segment 0 from the known context, lanes 1..3 nd run segment s >= 1
-// from every possible incoming context (lane 1 + (s - 1) nd + c), lane 31
-// holds the DEAD row. Each row carries the lane of the row the next segment
-// continues from, so resolving a round is three dependent shuffles -- no
-// shared rows, no barrier, no copies of the states. With tables of a few
-// KB, many streams share an SM.
+// Alphabets of up to kShflMaxNd symbols: every chain fits in one warp:
+// lane 0 runs segment 0 from the known context, lanes 1..3 nd run segment
+// s >= 1 from every possible incoming context (lane 1 + (s - 1) nd + c),
+// lane 31 holds the DEAD row. Each row carries the lane of the row the next
+// segment continues from, so resolving a round is three dependent shuffles
+// -- no shared rows, no barrier, no copies of the states. The columns are
+// packed (16 four-bit entries per u64; for NARROW, |D| <= 7, the low 32 bits
+// hold them all), so a chain step is a shift and a mask of a register
+// instead of a shared-memory load.
+template <bool NARROW>
 __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
                                           uint8_t *__restrict__ out, uint32_t lt) {
     const int lane = threadIdx.x & 31;
@@ -959,28 +993,45 @@ __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restric
     const uint32_t myseg = task ? (uint32_t)(1 + (lane - 1) / nd) : 0u;
     const uint32_t myc = task ? (uint32_t)((lane - 1) % nd) : 0u;
     const uint32_t nbase = 1u + myseg * (uint32_t)nd;  // lane of the next segment's context-0 row
-    const uint8_t *COL = I.COL;
+    const uint64_t *PK = reinterpret_cast<const uint64_t *>(I.COL);
     const uint32_t deadw = 0x01010101u * dead;
     uint32_t din = (uint32_t)S.start;
     const int seg = lane >> 3, pos = lane & 7;
     const uint32_t shd = 24u - 8u * (uint32_t)(pos & 3);
     const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);
 
-    auto resolve = [&](uint32_t, uint32_t cb, uint32_t &d, uint32_t &ctx) {
-        uint32_t sl[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, cb, 8 * myseg + k);
+    auto resolve = [&](uint32_t, uint64_t col, uint32_t &d, uint32_t &ctx) {
         uint32_t dd = lane == 0 ? din : myc;
         uint32_t hi = 0, lo = 0;
+        if constexpr (NARROW) {
+            uint32_t sl[8];
+            const uint32_t c32 = (uint32_t)col;
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            dd = COL[sl[k] + dd];
-            hi = hi * 256u + dd;
-        }
+            for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, c32, 8 * myseg + k);
 #pragma unroll
-        for (int k = 4; k < 8; k++) {
-            dd = COL[sl[k] + dd];
-            lo = lo * 256u + dd;
+            for (int k = 0; k < 4; k++) {
+                dd = (sl[k] >> (dd << 2)) & 15u;
+                hi = (hi << 8) | dd;
+            }
+#pragma unroll
+            for (int k = 4; k < 8; k++) {
+                dd = (sl[k] >> (dd << 2)) & 15u;
+                lo = (lo << 8) | dd;
+            }
+        } else {
+            uint64_t sl[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, col, 8 * myseg + k);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                dd = (uint32_t)(sl[k] >> (dd << 2)) & 15u;
+                hi = (hi << 8) | dd;
+            }
+#pragma unroll
+            for (int k = 4; k < 8; k++) {
+                dd = (uint32_t)(sl[k] >> (dd << 2)) & 15u;
+                lo = (lo << 8) | dd;
+            }
         }
         uint32_t nx = dd == dead ? 31u : nbase + dd;
         if (lane == 31) {
@@ -1005,29 +1056,33 @@ __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restric
         ctx = pos == 0 ? in : ((pos <= 4 ? row_x : row_y) >> shc) & 0xffu;
         din = r3y & 0xffu;
     };
-    return o1_rounds(S, R, out, lt, I.M, I.FC, I.DS, I.stride, dead, true, S.states[lane], resolve);
+    return o1_rounds(S, R, out, lt, PackedCols{I.M, PK}, I.FC, I.DS, I.stride, dead, true, S.states[lane],
+                     resolve);
 }
 
-// Wider alphabets (kSmallMaxNd < |D| <= kDenseMax) in one warp: lane 0 runs
-// segment 0; lanes 1-10, 11-20 and 21-30 run segments 1, 2 and 3, lane i of
-// a segment following the incoming contexts i, i + 10, ... (TPL chains per
-// lane, TPL = ceil(nd / 10), interleaved so their loads overlap). All chains
-// of a lane share one segment, so a round needs eight slot shuffles per
-// lane whatever TPL is. Rows go to a double-buffered shared array and are
-// resolved after a __syncwarp with three dependent loads, as in the
-// four-warp decoder, but without its barrier or its replicated states: one
-// warp and ~30 KB of shared memory per full-range quality stream, so several
-// streams share an SM.
+// Wider alphabets in one warp: lane 0 runs segment 0; lanes 1-10, 11-20 and
+// 21-30 run segments 1, 2 and 3, lane i of a segment following the incoming
+// contexts i, i + 10, ... (TPL chains per lane, TPL = ceil(nd / 10),
+// interleaved so their steps overlap). All chains of a lane share one
+// segment, so a round needs eight column shuffles per lane whatever TPL is.
+// Rows go to a double-buffered shared array (rows 0 .. 3 nd - 1, then the
+// DEAD row and a row for lanes without a task) and are resolved after a
+// __syncwarp with three dependent loads, as in the four-warp decoder, but
+// without its barrier or its replicated states: one warp and ~30 KB of
+// shared memory per full-range quality stream, so several streams share an
+// SM. PACKED (|D| <= kSmallMaxNd) steps chains in registers on packed
+// columns; otherwise a step is a byte load from a column.
 constexpr int kWideLanes = 10;  // lanes per speculative segment
 
-template <int TPL>
+template <int TPL, bool PACKED>
 __device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
-                                          uint4 (*__restrict__ rows)[kOutRows + 1], uint8_t *__restrict__ out,
-                                          uint32_t lt) {
+                                          uint4 *__restrict__ rows0, uint4 *__restrict__ rows1,
+                                          uint8_t *__restrict__ out, uint32_t lt) {
     const int lane = threadIdx.x & 31;
     const int nd = S.nd;
     const DenseImage I(sm, nd);
     const uint32_t dead = I.dead;
+    const uint32_t deadrow = 3u * (uint32_t)nd, padrow = deadrow + 1u;
     const bool worker = lane >= 1 && lane <= 3 * kWideLanes;
     const uint32_t myseg = worker ? (uint32_t)(1 + (lane - 1) / kWideLanes) : 0u;
     const uint32_t li = worker ? (uint32_t)((lane - 1) % kWideLanes) : 0u;
@@ -1038,13 +1093,13 @@ __device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restric
         const uint32_t c = li + kWideLanes * q;
         const bool valid = worker && c < (uint32_t)nd;
         c_q[q] = valid ? c : 0u;
-        idx_q[q] = valid ? (myseg - 1) * (uint32_t)nd + c : kPadRow;
+        idx_q[q] = valid ? (myseg - 1) * (uint32_t)nd + c : padrow;
     }
     const uint8_t *COL = I.COL;
     const uint32_t deadw = 0x01010101u * dead;
     if (lane == 0) {
-        rows[0][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
-        rows[1][kDeadRow] = make_uint4(deadw, deadw, kDeadRow * 16u, 0u);
+        rows0[deadrow] = make_uint4(deadw, deadw, deadrow * 16u, 0u);
+        rows1[deadrow] = make_uint4(deadw, deadw, deadrow * 16u, 0u);
     }
     __syncwarp();
     uint32_t din = (uint32_t)S.start;
@@ -1053,8 +1108,9 @@ __device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restric
     const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);
     uint32_t buf = 0;
 
-    auto resolve = [&](uint32_t, uint32_t cb, uint32_t &d, uint32_t &ctx) {
-        uint32_t sl[8];
+    auto resolve = [&](uint32_t, auto cb, uint32_t &d, uint32_t &ctx) {
+        using CT = decltype(cb);
+        CT sl[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) sl[k] = __shfl_sync(0xffffffffu, cb, 8 * myseg + k);
         uint32_t dd[TPL], hi[TPL], lo[TPL];
@@ -1065,31 +1121,25 @@ __device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restric
             lo[q] = 0;
         }
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < 8; k++) {
 #pragma unroll
             for (int q = 0; q < TPL; q++) {
-                dd[q] = COL[sl[k] + dd[q]];
-                hi[q] = hi[q] * 256u + dd[q];
+                if constexpr (PACKED) dd[q] = (uint32_t)(sl[k] >> (dd[q] << 2)) & 15u;
+                else dd[q] = COL[sl[k] + dd[q]];
+                if (k < 4) hi[q] = (hi[q] << 8) | dd[q];
+                else lo[q] = (lo[q] << 8) | dd[q];
             }
         }
-#pragma unroll
-        for (int k = 4; k < 8; k++) {
-#pragma unroll
-            for (int q = 0; q < TPL; q++) {
-                dd[q] = COL[sl[k] + dd[q]];
-                lo[q] = lo[q] * 256u + dd[q];
-            }
-        }
-        uint4 *rb = rows[buf];
+        uint4 *rb = buf ? rows1 : rows0;
 #pragma unroll
         for (int q = 0; q < TPL; q++) {
-            const uint32_t nx = 16u * (dd[q] == dead ? kDeadRow : nbase + dd[q]);
+            const uint32_t nx = 16u * (dd[q] == dead ? deadrow : nbase + dd[q]);
             if (q > 0 || lane != 0) rb[idx_q[q]] = make_uint4(hi[q], lo[q], nx, 0u);
         }
         uint4 r0;
         r0.x = __shfl_sync(0xffffffffu, hi[0], 0);
         r0.y = __shfl_sync(0xffffffffu, lo[0], 0);
-        r0.z = __shfl_sync(0xffffffffu, 16u * (dd[0] == dead ? kDeadRow : nbase + dd[0]), 0);
+        r0.z = __shfl_sync(0xffffffffu, 16u * (dd[0] == dead ? deadrow : nbase + dd[0]), 0);
         __syncwarp();
         const uint8_t *rbb = reinterpret_cast<const uint8_t *>(rb);
         const uint4 r1 = *reinterpret_cast<const uint4 *>(rbb + r0.z);
@@ -1106,20 +1156,27 @@ __device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restric
         din = r3.y & 0xffu;
         buf ^= 1u;
     };
-    return o1_rounds(S, R, out, lt, I.M, I.FC, I.DS, I.stride, dead, true, S.states[lane], resolve);
+    if constexpr (PACKED)
+        return o1_rounds(S, R, out, lt, PackedCols{I.M, reinterpret_cast<const uint64_t *>(I.COL)}, I.FC, I.DS,
+                         I.stride, dead, true, S.states[lane], resolve);
+    else
+        return o1_rounds(S, R, out, lt, ByteCols{I.M}, I.FC, I.DS, I.stride, dead, true, S.states[lane], resolve);
 }
 
-// The two one-warp order-1 decoders: `wide` selects o1w_stream (rows in
-// shared memory, TPL chains per lane) over o1s_stream.
+// The two one-warp order-1 decoders: the small class (packed columns:
+// o1s_stream up to kShflMaxNd symbols, o1w_stream<2, packed> up to
+// kSmallMaxNd) and the wide class (byte columns, o1w_stream<TPL>). Row
+// arrays: 3 nd + 2 rows per buffer.
 template <bool kWide>
 __global__ void __launch_bounds__(32)
     dec_o1w_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
                    uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off,
                    uint32_t first_polls) {
+    constexpr int kRows = 3 * (kWide ? kDenseMax : kSmallMaxNd) + 2;
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ __align__(16) uint4 s_rows[kWide ? 2 : 1][kWide ? kOutRows + 1 : 1];
+    __shared__ __align__(16) uint4 s_rows[2][kRows];
     const int lane = threadIdx.x;
     const uint32_t lt = lanemask_lt();
     TableStager st;
@@ -1145,18 +1202,22 @@ __global__ void __launch_bounds__(32)
         int status;
         if constexpr (kWide) {
             const int tpl = (S.nd + kWideLanes - 1) / kWideLanes;
-            status = tpl <= 2   ? o1w_stream<2>(S, sm, R, s_rows, out, lt)
-                     : tpl == 3 ? o1w_stream<3>(S, sm, R, s_rows, out, lt)
-                     : tpl == 4 ? o1w_stream<4>(S, sm, R, s_rows, out, lt)
-                                : o1w_stream<5>(S, sm, R, s_rows, out, lt);
+            status = tpl <= 2   ? o1w_stream<2, false>(S, sm, R, s_rows[0], s_rows[1], out, lt)
+                     : tpl == 3 ? o1w_stream<3, false>(S, sm, R, s_rows[0], s_rows[1], out, lt)
+                     : tpl == 4 ? o1w_stream<4, false>(S, sm, R, s_rows[0], s_rows[1], out, lt)
+                                : o1w_stream<5, false>(S, sm, R, s_rows[0], s_rows[1], out, lt);
         } else {
-            status = o1s_stream(S, sm, R, out, lt);
+            status = S.nd <= 7            ? o1s_stream<true>(S, sm, R, out, lt)
+                     : S.nd <= kShflMaxNd ? o1s_stream<false>(S, sm, R, out, lt)
+                                          : o1w_stream<2, true>(S, sm, R, s_rows[0], s_rows[1], out, lt);
         }
         if (lane == 0) S.status = status;
         __syncwarp();
     }
 }
 static_assert((kDenseMax + kWideLanes - 1) / kWideLanes <= 5, "o1w_stream instantiations cover TPL <= 5");
+static_assert((kSmallMaxNd + kWideLanes - 1) / kWideLanes <= 2, "the small class runs o1w_stream<2>");
+static_assert(3 * kShflMaxNd + 1 <= 31, "shuffle-resolved chains fit in a warp");
 
 // ---------------------------------------------------------------------------
 // order-1, large alphabets: tables stay in global memory (L2), one dependent

@@ -93,12 +93,15 @@ struct DecStream {
 
 enum { kClsNone = 0, kClsO0 = 1, kClsO1Dense = 2, kClsO1Global = 3 };
 // Launch classes of dense streams decoded by one warp each: |D| <=
-// kSmallMaxNd (every chain in its own lane) and wider alphabets (up to five
-// chains per lane). kClsO1Dense is then the four-warp decoder of the same
-// tables.
+// kSmallMaxNd (packed columns, chains stepped in registers) and wider
+// alphabets (byte columns, up to five chains per lane). kClsO1Dense is the
+// four-warp decoder of the byte columns.
 constexpr int kClsO1Small = 4;
 constexpr int kClsO1Wide = 5;
-constexpr int kSmallMaxNd = 10;
+constexpr int kSmallMaxNd = 15;
+// Up to this |D| every chain of a round has its own lane (3 |D| + 1 <= 31)
+// and rows are resolved by shuffles; above it rows go through shared memory.
+constexpr int kShflMaxNd = 10;
 
 // Decode table arena per stream (bytes from tbl_off).
 //   order-0: 4096 x u32 packed ((freq - 1) << 20) | ((slot - cum) << 8) | sym.
@@ -119,6 +122,9 @@ constexpr int kSmallMaxNd = 10;
 //                               for rows of absent contexts and for DEAD)
 //     Full-range quality tables (|D| ~ 31) have ~480 columns: ~28 KB against
 //     ~130 KB for a slot -> symbol table per context.
+//     Packed form, |D| <= kSmallMaxNd: M holds the column index j, and the
+//     columns are u64 at col_off, entry d in bits [4d, 4d + 4), so a chain
+//     step is a shift of a register instead of a shared-memory load.
 //   order-1 global (more symbols, or more columns than the image holds):
 //     [256 B] raw context -> dense index (0xFF absent), then per present
 //     context t: 4096 x u16 (sym << 8) | dense(sym), then 256 x u32
@@ -131,8 +137,17 @@ __host__ __device__ inline uint32_t dense_fc_bytes(int nd) {
     return (uint32_t)(((nd + 1) * (nd + 1) * 4 + 15) / 16 * 16);
 }
 __host__ __device__ inline uint32_t dense_col_off(int nd) { return kDenseM + dense_fc_bytes(nd) + 256; }
+__host__ __device__ inline bool dense_packed(int nd) { return nd <= kSmallMaxNd; }
+// Bytes of the table image (what is staged into shared memory).
 __host__ __device__ inline uint32_t dense_table_bytes(int nd, uint32_t ncol) {
-    return dense_col_off(nd) + ncol * dense_col_stride(nd);
+    return dense_packed(nd) ? dense_col_off(nd) + (8 * ncol + 15) / 16 * 16
+                            : dense_col_off(nd) + ncol * dense_col_stride(nd);
+}
+// Bytes the parse needs in the arena while building the image: the packed
+// form is built from byte columns placed after it.
+__host__ __device__ inline uint32_t dense_build_bytes(int nd, uint32_t ncol) {
+    return dense_packed(nd) ? dense_table_bytes(nd, ncol) + ncol * dense_col_stride(nd)
+                            : dense_table_bytes(nd, ncol);
 }
 constexpr uint64_t kDecCtxMap = 0;
 constexpr uint64_t kDecO1Base = 256;
