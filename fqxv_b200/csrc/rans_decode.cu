@@ -1039,12 +1039,17 @@ __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restric
             lo = deadw;
             nx = 31u;
         }
+        // Three levels of shuffles: every lane first learns the row two
+        // segments on (nn, the next of its next); then lane 0's row gives
+        // the rows of segments 1 and 2 at once (n0, and n1 = nn of lane 0),
+        // and those give the rows of segments 2 and 3 (n2 = nn of lane n0).
+        const uint32_t nn = __shfl_sync(0xffffffffu, nx, nx);
         const uint32_t r0x = __shfl_sync(0xffffffffu, hi, 0), r0y = __shfl_sync(0xffffffffu, lo, 0);
         const uint32_t n0 = __shfl_sync(0xffffffffu, nx, 0);
+        const uint32_t n1 = __shfl_sync(0xffffffffu, nn, 0);
         const uint32_t r1x = __shfl_sync(0xffffffffu, hi, n0), r1y = __shfl_sync(0xffffffffu, lo, n0);
-        const uint32_t n1 = __shfl_sync(0xffffffffu, nx, n0);
+        const uint32_t n2 = __shfl_sync(0xffffffffu, nn, n0);
         const uint32_t r2x = __shfl_sync(0xffffffffu, hi, n1), r2y = __shfl_sync(0xffffffffu, lo, n1);
-        const uint32_t n2 = __shfl_sync(0xffffffffu, nx, n1);
         const uint32_t rx = seg == 0 ? r0x : seg == 1 ? r1x : r2x;
         const uint32_t ry = seg == 0 ? r0y : seg == 1 ? r1y : r2y;
         const uint32_t ine = seg == 0 ? din : seg == 1 ? (r0y & 0xffu) : (r1y & 0xffu);

@@ -385,6 +385,96 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
     state = x;
 }
 
+// Order-1 reverse encode without a per-position key array (scalar.rs:84-90):
+// the context of position i is byte i - 1, which for lanes 1-31 is the
+// symbol the lane below holds in the same round, and for lane 0 the symbol
+// lane 31 holds one round lower -- one shuffle per round instead of a second
+// byte load. A chunk's table entries (dense index of the context and the
+// symbol, then the table) are computed while the chunk above it runs its
+// state chain, from symbols loaded two chunks ahead, so neither the loads nor
+// the lookups stand between one chunk's chain and the next.
+template <bool SMEM_TAB>
+__device__ __forceinline__ void encode_warp_o1(const uint8_t *__restrict__ p, uint64_t n,
+                                               const uint2 *__restrict__ tab, const uint8_t *__restrict__ umap,
+                                               uint32_t nu, uint16_t *__restrict__ words, uint64_t word_end,
+                                               uint64_t &nwords, uint32_t &state) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    const uint32_t below = (uint32_t)(lane + 31) & 31u;  // the lane holding the byte before this lane's
+    uint32_t x = kRansL;
+    uint16_t *wptr = words + word_end;
+    const int64_t full = (int64_t)(n / 32);
+    const uint32_t rem = (uint32_t)(n % 32);
+    auto tabat = [&](uint32_t idx) -> uint2 { return SMEM_TAB ? tab[idx] : __ldg(tab + idx); };
+    auto sym = [&](int64_t r) -> uint32_t { return r >= 0 ? (uint32_t)__ldg(p + (uint64_t)r * 32 + lane) : 0u; };
+    if (rem) {
+        const uint64_t i = (uint64_t)full * 32 + lane;
+        const bool active = lane < (int)rem;
+        const uint32_t s = active ? (uint32_t)__ldg(p + i) : 0u;
+        const uint32_t prev = (active && i > 0) ? (uint32_t)__ldg(p + i - 1) : 0u;
+        const uint2 e = active ? tabat((uint32_t)umap[prev] * nu + umap[s]) : make_uint2(0u, 0u);
+        const uint32_t x_before = x;
+        const bool need = enc_step(x, e, active);
+        enc_emit(need, x_before, wptr, lt);
+    }
+    // entries of the chunk whose top round is rt, from its symbols cs[k]
+    // (round rt - k) and the symbol of round rt - 16 (lane 31's is the
+    // context of lane 0 in round rt - 15); rounds below 0 hold symbol 0,
+    // which is the context of position 0
+    auto entries = [&](const uint32_t (&cs)[16], uint32_t low, uint2 (&ent)[16]) {
+        uint32_t u[17];
+#pragma unroll
+        for (int k = 0; k < 16; k++) u[k] = umap[cs[k]];
+        u[16] = umap[low];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const uint32_t up = __shfl_sync(0xffffffffu, lane == 31 ? u[k + 1] : u[k], below);
+            ent[k] = tabat(up * nu + u[k]);
+        }
+    };
+    uint32_t c1[16], c2[16], wv[16], pwv[16];
+    uint2 ent[16], entn[16];
+    uint32_t pbits = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        c1[k] = sym(full - 1 - k);
+        pwv[k] = 0;
+    }
+    {
+        uint32_t c0[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) c0[k] = c1[k];
+#pragma unroll
+        for (int k = 0; k < 16; k++) c1[k] = sym(full - 17 - k);
+        entries(c0, c1[0], ent);
+    }
+    for (int64_t rt = full - 1; rt >= 0; rt -= 16) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) c2[k] = sym(rt - 32 - k);
+        entries(c1, c2[0], entn);
+        const bool whole = rt >= 15;
+        uint32_t bits = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            wv[k] = x;
+            const bool active = whole || k <= rt;
+            if (enc_step(x, ent[k], active)) bits |= 1u << k;
+            enc_emit((pbits >> k) & 1u, pwv[k], wptr, lt);
+        }
+        pbits = bits;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            ent[k] = entn[k];
+            c1[k] = c2[k];
+            pwv[k] = wv[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k++) enc_emit((pbits >> k) & 1u, pwv[k], wptr, lt);
+    nwords = (uint64_t)((words + word_end) - wptr);
+    state = x;
+}
+
 // Order-1 tables of alphabets up to kEncO1SmemNu symbols are copied into
 // the warp's slice of dynamic shared memory; larger ones are read through L1.
 constexpr uint32_t kEncO1SmemNu = 45;
@@ -431,14 +521,14 @@ __global__ void __launch_bounds__(kEncWarpsPerCta * 32)
                         encode_warp<1, true, true>(p, n, t, s_umap[warp], nu, keys + ((uintptr_t)src & 15u) + B.src_off, words,
                                                    word_end, nw, st);
                     else
-                        encode_warp<1, true, false>(p, n, t, s_umap[warp], nu, nullptr, words, word_end, nw, st);
+                        encode_warp_o1<true>(p, n, t, s_umap[warp], nu, words, word_end, nw, st);
                 } else {
                     __syncwarp();
                     if (keys)
                         encode_warp<1, false, true>(p, n, T1, s_umap[warp], nu, keys + ((uintptr_t)src & 15u) + B.src_off, words,
                                                     word_end, nw, st);
                     else
-                        encode_warp<1, false, false>(p, n, T1, s_umap[warp], nu, nullptr, words, word_end, nw, st);
+                        encode_warp_o1<false>(p, n, T1, s_umap[warp], nu, words, word_end, nw, st);
                 }
             }
         }

@@ -37,6 +37,11 @@ from . import workloads as W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
+# the library's built-in rules (csrc/rans_ctx.cuh, struct Tuning)
+DEFAULTS = {"o1_four_max_streams": -1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
+            "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "dense_edge_small": 40 << 10,
+            "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 16}
+
 
 def _batch(kind: str, nblocks: int, block: int, seed: int):
     blobs = [W.GENERATORS[kind](block, seed + i) if kind != "ont" else W.ont_reads(block // 8000 + 2, seed + i)[:block]
@@ -129,10 +134,12 @@ def sweep(reps: int = 3) -> dict:
             row[name] = b.decode_gbs(reps)
         wide[count] = row
         del b
-    crossover = next((k for k in sorted(wide) if wide[k]["wide"] >= wide[k]["four"]), 1 << 30)
-    params["o1_four_max_streams"] = int(crossover)
-    c.set_param("o1_four_max_streams", crossover)
     meas["gbs_o1_wide_vs_four_by_streams"] = {str(k): {n: round(g, 3) for n, g in v.items()} for k, v in wide.items()}
+    # ... but the rule is chosen on a mix of config 2's stream types and sizes,
+    # where the longest streams bound a launch group rather than its count
+    mix, mspans, _ = W.config2(nblocks=1024, hi=4 << 20, seed=700)
+    bm = Bench(c, mix, mspans, 2)
+    pick("o1_four_max_streams", (0, sms // 2, sms, 2 * sms, 4 * sms, 1 << 30), lambda: bm.decode_gbs(reps))
 
     caps = (1, 2, 4, 8, 16, 32)
     b = Bench(c, *_batch("binned", 1024, 256 << 10, 200), 0)
@@ -170,6 +177,18 @@ def sweep(reps: int = 3) -> dict:
     b = Bench(c, data, spans, 2)
     pick("enc_run_ctas_per_sm", (4, 8, 16, 32), lambda: b.encode_gbs(reps))
     del b
+    # the whole table against the built-in rules on the mix: decode
+    # parameters fall back to the built-in ones when the table is slower
+    tuned = bm.decode_gbs(reps)
+    for k, v in DEFAULTS.items():
+        c.set_param(k, v)
+    builtin = bm.decode_gbs(reps)
+    meas["gbs_mix_decode_table_vs_builtin"] = {"table": round(tuned, 3), "builtin": round(builtin, 3)}
+    if builtin > tuned:
+        for k in DEFAULTS:
+            if k != "enc_run_ctas_per_sm":
+                params.pop(k, None)
+    del bm
     c.close()
     return {"device": dev.name, "sm_count": sms, "params": params, "measurements": meas,
             "when": time.strftime("%Y-%m-%d %H:%M:%S")}
