@@ -279,16 +279,20 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     CK(cudaMemcpyAsync(hst, dS, szs, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     {
-        // Launch groups: order-0; order-1 dense by alphabet size (the shared
-        // memory of a group is its largest member's, so small alphabets get
-        // many CTAs per SM; the smallest decode with one warp per stream);
-        // order-1 global.
+        // Launch groups: order-0; order-1 small alphabets (one warp per
+        // stream, many per SM); order-1 byte columns by table size (the
+        // shared memory of a group is its largest member's), with the
+        // largest of those streams in a group of their own on the four-warp
+        // decoder (`ord` runs largest first); order-1 global.
         const DecStream *ps = reinterpret_cast<const DecStream *>(hst);
+        const int64_t four_top = ctx->tune.o1_four_top < 0 ? ctx->sms / 2 : ctx->tune.o1_four_top;
+        int64_t wide_seen = 0;
         auto group_of = [&](const DecStream &d) -> int {
             if (d.cls == kClsO0) return 0;
             if (d.cls == kClsO1Global) return kGroups - 1;
             if (d.cls != kClsO1Dense) return -1;
             if (d.nd <= kSmallMaxNd) return 1;
+            if (wide_seen++ < four_top) return kGroupFourTop;
             return d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_small   ? 2
                    : d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_large ? 3
                                                                          : 4;
@@ -312,6 +316,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             if (g == 0) gcls[g] = kClsO0;
             else if (g == kGroups - 1) gcls[g] = kClsO1Global;
             else if (g == 1) gcls[g] = kClsO1Small;
+            else if (g == kGroupFourTop) gcls[g] = kClsO1Dense;
             else gcls[g] = (int64_t)lists[g].size() < four_max ? kClsO1Dense : kClsO1Wide;
             smem[g] = dec_smem_bytes(gcls[g], tmax[g]);
         }

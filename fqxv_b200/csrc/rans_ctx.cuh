@@ -72,7 +72,11 @@ struct HostBuf {
     }
 };
 
-constexpr int kGroups = 6;  // decode launch groups
+// Decode launch groups: order-0; order-1 small alphabets; order-1 byte
+// columns in three table-size ranges; the largest order-1 byte-column
+// streams (four-warp decoder); order-1 global tables.
+constexpr int kGroups = 7;
+constexpr int kGroupFourTop = 5;
 
 enum Stage {
     kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
@@ -92,6 +96,11 @@ struct Tuning {
     // decoder (one stream per SM), larger groups to the one-warp decoder
     // (several per SM). -1: the SM count.
     int64_t o1_four_max_streams = -1;
+    // The this-many largest of those streams in a batch form a launch group
+    // of their own on the four-warp decoder, whatever the group sizes: a
+    // batch lasts at least as long as its longest serial chain. -1: half the
+    // SM count.
+    int64_t o1_four_top = -1;
     // CTAs per SM of each decode class, at most (the occupancy API bounds it too)
     int64_t cta_cap_o0 = 32, cta_cap_o1_small = 32, cta_cap_o1_wide = 32, cta_cap_o1_four = 8,
             cta_cap_o1_global = 32;

@@ -34,6 +34,7 @@ struct ParamDef {
 
 const ParamDef kParams[] = {
     {"o1_four_max_streams", &Tuning::o1_four_max_streams, -1, 1 << 30},
+    {"o1_four_top", &Tuning::o1_four_top, -1, 1 << 30},
     {"cta_cap_o0", &Tuning::cta_cap_o0, 1, 64},
     {"cta_cap_o1_small", &Tuning::cta_cap_o1_small, 1, 64},
     {"cta_cap_o1_wide", &Tuning::cta_cap_o1_wide, 1, 64},

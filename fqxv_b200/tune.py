@@ -10,6 +10,9 @@ checked byte for byte against the input on every measurement. The
 reference's only run-time choice is its SIMD backend
 (crates/fqxv-rans/src/lib.rs:80-97); these are the GPU's counterparts:
 
+  o1_four_top           the largest this-many wide-alphabet order-1 streams of
+                        a batch decode on the four-warp decoder, in a launch
+                        group of their own
   o1_four_max_streams   below this many wide-alphabet order-1 streams in a
                         launch group the four-warp decoder (one stream per
                         SM, lower latency per stream) runs them, else the
@@ -38,7 +41,7 @@ from . import workloads as W
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # the library's built-in rules (csrc/rans_ctx.cuh, struct Tuning)
-DEFAULTS = {"o1_four_max_streams": -1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
+DEFAULTS = {"o1_four_max_streams": -1, "o1_four_top": -1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
             "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "dense_edge_small": 40 << 10,
             "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 16}
 
@@ -139,6 +142,7 @@ def sweep(reps: int = 3) -> dict:
     # where the longest streams bound a launch group rather than its count
     mix, mspans, _ = W.config2(nblocks=1024, hi=4 << 20, seed=700)
     bm = Bench(c, mix, mspans, 2)
+    pick("o1_four_top", (0, sms // 4, sms // 2, sms), lambda: bm.decode_gbs(reps))
     pick("o1_four_max_streams", (0, sms // 2, sms, 2 * sms, 4 * sms, 1 << 30), lambda: bm.decode_gbs(reps))
 
     caps = (1, 2, 4, 8, 16, 32)

@@ -10,6 +10,7 @@ from conftest import ROOT
 
 KNOWN = {
     "o1_four_max_streams": (-1, 1 << 30),
+    "o1_four_top": (-1, 1 << 30),
     "cta_cap_o0": (1, 64),
     "cta_cap_o1_small": (1, 64),
     "cta_cap_o1_wide": (1, 64),
