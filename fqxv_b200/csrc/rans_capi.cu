@@ -121,7 +121,7 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     // model and read by the encode
     uint64_t src_end = 0;
     for (size_t i = 0; i < nb; i++) src_end = std::max<uint64_t>(src_end, blocks[i].offset + blocks[i].length);
-    const bool keyed = o1 && ctx->enc_keys;
+    const bool keyed = o1 && ctx->tune.enc_o1_keys;
     if (keyed) CK(ctx->e_keys.ensure(2 * (src_end + 16), s));
     uint16_t *dK = keyed ? ctx->e_keys.as<uint16_t>() : nullptr;
     CK(ctx->e_misc.ensure((2 + nb) * 16, s));
@@ -286,13 +286,33 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         // decoder (`ord` runs largest first); order-1 global.
         const DecStream *ps = reinterpret_cast<const DecStream *>(hst);
         const int64_t four_top = ctx->tune.o1_four_top < 0 ? ctx->sms / 2 : ctx->tune.o1_four_top;
-        int64_t wide_seen = 0;
+        const int64_t small_top = ctx->tune.o1_small_top < 0 ? ctx->sms / 2 : ctx->tune.o1_small_top;
+        // A stream whose serial decode (its rounds one after another) takes
+        // longer than o1_top_latency_pct % of the whole batch's throughput-
+        // bound time would finish last however the rest is packed: such
+        // order-1 streams (up to the counts above) form the top groups.
+        // Costs in SM cycles per byte, from B200 measurements: a stream's
+        // latency is cycles per 32-byte round / 32; the batch's throughput
+        // time is the sum over streams of bytes x (SM cycles per byte at the
+        // class's full-GPU rate) / SMs.
+        auto lat_cpb = [](const DecStream &d) {
+            return d.cls == kClsO0 ? 5.0 : d.nd <= kShflMaxNd ? 15.0 : d.nd <= kSmallMaxNd ? 18.0 : 19.5;
+        };
+        auto rate_cpb = [](const DecStream &d) {
+            return d.cls == kClsO0 ? 0.9 : d.cls == kClsO1Global ? 14.0 : d.nd <= kSmallMaxNd ? 3.0 : 7.0;
+        };
+        double bulk = 0;
+        for (size_t i = 0; i < nb; i++)
+            if (ps[i].cls != kClsNone) bulk += (double)ps[i].n * rate_cpb(ps[i]);
+        const double top_thr = bulk / ctx->sms * (double)ctx->tune.o1_top_latency_pct / 100.0;
+        int64_t wide_seen = 0, small_seen = 0;
         auto group_of = [&](const DecStream &d) -> int {
             if (d.cls == kClsO0) return 0;
             if (d.cls == kClsO1Global) return kGroups - 1;
             if (d.cls != kClsO1Dense) return -1;
-            if (d.nd <= kSmallMaxNd) return 1;
-            if (wide_seen++ < four_top) return kGroupFourTop;
+            const bool top = (double)d.n * lat_cpb(d) > top_thr;
+            if (d.nd <= kSmallMaxNd) return top && small_seen++ < small_top ? kGroupSmallTop : 1;
+            if (top && wide_seen++ < four_top) return kGroupFourTop;
             return d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_small   ? 2
                    : d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_large ? 3
                                                                          : 4;
@@ -315,10 +335,13 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         for (int g = 0; g < kGroups; g++) {
             if (g == 0) gcls[g] = kClsO0;
             else if (g == kGroups - 1) gcls[g] = kClsO1Global;
-            else if (g == 1) gcls[g] = kClsO1Small;
+            else if (g == 1 || g == kGroupSmallTop) gcls[g] = kClsO1Small;
             else if (g == kGroupFourTop) gcls[g] = kClsO1Dense;
             else gcls[g] = (int64_t)lists[g].size() < four_max ? kClsO1Dense : kClsO1Wide;
             smem[g] = dec_smem_bytes(gcls[g], tmax[g]);
+            // the groups of largest streams: one CTA per SM, alone on it
+            if ((g == kGroupFourTop || g == kGroupSmallTop) && ctx->tune.o1_top_exclusive)
+                smem[g] = std::max(smem[g], dec_exclusive_smem(gcls[g]));
         }
         // Groups are launched longest first -- by the serial time of their
         // largest stream (rounds x cycles per round: ~620 for order-1,
@@ -503,11 +526,20 @@ int fqxv_rans_ctx_create(int device, fqxv_rans_ctx **out) {
         else if (!std::strcmp(e, "four")) c->tune.o1_four_max_streams = 1 << 30;
     }
     // FQXV_RANS_ENC_KEYS=0: order-1 encode without the per-position key array.
-    if (const char *e = std::getenv("FQXV_RANS_ENC_KEYS")) c->enc_keys = std::strcmp(e, "0") != 0;
+    if (const char *e = std::getenv("FQXV_RANS_ENC_KEYS")) c->tune.enc_o1_keys = std::strcmp(e, "0") != 0;
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    // The groups of largest streams go on the highest-priority streams, so
+    // their CTAs are placed before the rest of the batch fills the SMs.
+    int prio_lo = 0, prio_hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) {
+        cudaGetLastError();
+        prio_lo = prio_hi = 0;
+    }
     for (int i = 0; i < kGroups && ok; i++)
-        ok = cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking) == cudaSuccess &&
+        ok = cudaStreamCreateWithPriority(&c->aux[i], cudaStreamNonBlocking,
+                                          i == kGroupFourTop || i == kGroupSmallTop ? prio_hi : prio_lo) ==
+                 cudaSuccess &&
              cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();

@@ -74,9 +74,11 @@ struct HostBuf {
 
 // Decode launch groups: order-0; order-1 small alphabets; order-1 byte
 // columns in three table-size ranges; the largest order-1 byte-column
-// streams (four-warp decoder); order-1 global tables.
-constexpr int kGroups = 7;
+// streams (four-warp decoder) and the largest small-alphabet ones, each of
+// these two on SMs of their own; order-1 global tables.
+constexpr int kGroups = 8;
 constexpr int kGroupFourTop = 5;
+constexpr int kGroupSmallTop = 6;
 
 enum Stage {
     kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
@@ -96,11 +98,19 @@ struct Tuning {
     // decoder (one stream per SM), larger groups to the one-warp decoder
     // (several per SM). -1: the SM count.
     int64_t o1_four_max_streams = -1;
-    // The this-many largest of those streams in a batch form a launch group
-    // of their own on the four-warp decoder, whatever the group sizes: a
-    // batch lasts at least as long as its longest serial chain. -1: half the
+    // Order-1 streams whose serial decode alone outlasts o1_top_latency_pct %
+    // of the batch's throughput-bound time form launch groups of their own
+    // (the batch lasts at least as long as its longest serial chain): wide
+    // alphabets on the four-warp decoder, at most o1_four_top streams, small
+    // alphabets on the one-warp decoder, at most o1_small_top. -1: half the
     // SM count.
+    int64_t o1_top_latency_pct = 75;
     int64_t o1_four_top = -1;
+    int64_t o1_small_top = -1;
+    // 1: those two groups run one CTA per SM with no other CTA beside it
+    // (their CTAs claim the SM's shared memory), so their serial chains are
+    // not slowed by the rest of the batch; 0: they share.
+    int64_t o1_top_exclusive = 1;
     // CTAs per SM of each decode class, at most (the occupancy API bounds it too)
     int64_t cta_cap_o0 = 32, cta_cap_o1_small = 32, cta_cap_o1_wide = 32, cta_cap_o1_four = 8,
             cta_cap_o1_global = 32;
@@ -108,6 +118,10 @@ struct Tuning {
     int64_t dense_edge_small = 40 << 10, dense_edge_large = 80 << 10;
     // encode kernel grid, CTAs per SM
     int64_t enc_run_ctas_per_sm = 16;
+    // Order-1 encode: 1, the model kernel stores each position's table index
+    // (u16) for the encode kernel to read back; 0, the encode kernel derives
+    // it from the byte and its predecessor (no per-position array).
+    int64_t enc_o1_keys = 1;
     std::string source;  // the table file applied (empty: defaults)
 };
 int tuning_set(Tuning &t, const char *key, int64_t value);
@@ -262,10 +276,6 @@ struct fqxv_rans_ctx {
     // setter in fqxv_rans_gpu_testing.h lowers it.
     uint32_t first_polls = fqxv::kWaitPolls;
     fqxv::Tuning tune;
-    // Order-1 encode: the model kernel stores each position's table index
-    // (u16) for the encode kernel to read back, instead of the encode
-    // kernel deriving it from the byte and its predecessor.
-    bool enc_keys = true;
     // arenas of the extended-format calls (rans_x.cu), created on first use
     // and freed by fqxv::x_release
     void *xb = nullptr;

@@ -23,6 +23,7 @@
 //      memory reads per round instead of 32).
 // Malformed input never faults: every read of the stream is bounds checked
 // and errors are reported per stream as the reference's Malformed kinds.
+#include <algorithm>
 #include <mutex>
 
 #include "rans_common.cuh"
@@ -1319,6 +1320,26 @@ uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes) {
     }
 }
 
+// Dynamic shared memory of one CTA that leaves no room on its SM for any
+// other: the per-block opt-in maximum less the kernel's static shared memory.
+static uint32_t exclusive_bytes(const void *fn) {
+    int dev = 0, optin = 0;
+    cudaFuncAttributes a;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&a, fn) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return optin > (int)a.sharedSizeBytes ? (uint32_t)(optin - (int)a.sharedSizeBytes) / 128 * 128 : 0u;
+}
+
+uint32_t dec_exclusive_smem(int cls) {
+    if (cls == kClsO1Dense) return exclusive_bytes(reinterpret_cast<const void *>(dec_o1d_kernel));
+    if (cls == kClsO1Small) return exclusive_bytes(reinterpret_cast<const void *>(dec_o1w_kernel<false>));
+    return 0;
+}
+
 // Each decode kernel's dynamic shared-memory limit is raised once per
 // device to the largest size any launch uses. Setting it per launch would
 // race between host threads that launch the same kernel with different sizes
@@ -1337,11 +1358,11 @@ static void ensure_dec_attrs() {
     cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)dec_smem_bytes(kClsO0, 0));
     cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)dec_smem_bytes(kClsO1Dense, kDenseImageMax));
+                         (int)std::max(dec_smem_bytes(kClsO1Dense, kDenseImageMax), dec_exclusive_smem(kClsO1Dense)));
     cudaFuncSetAttribute(dec_o1g_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)dec_smem_bytes(kClsO1Global, 0));
     cudaFuncSetAttribute(dec_o1w_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)dec_smem_bytes(kClsO1Small, kDenseImageMax));
+                         (int)std::max(dec_smem_bytes(kClsO1Small, kDenseImageMax), dec_exclusive_smem(kClsO1Small)));
     cudaFuncSetAttribute(dec_o1w_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)dec_smem_bytes(kClsO1Wide, kDenseImageMax));
     g_attr_done[dev] = true;

@@ -391,8 +391,9 @@ __device__ __forceinline__ void encode_warp(const uint8_t *__restrict__ p, uint6
 // lane 31 holds one round lower -- one shuffle per round instead of a second
 // byte load. A chunk's table entries (dense index of the context and the
 // symbol, then the table) are computed while the chunk above it runs its
-// state chain, from symbols loaded two chunks ahead, so neither the loads nor
-// the lookups stand between one chunk's chain and the next.
+// state chain, from symbols loaded one chunk earlier (the byte below a
+// chunk's lowest round too), so neither the loads nor the lookups stand
+// between one chunk's chain and the next.
 template <bool SMEM_TAB>
 __device__ __forceinline__ void encode_warp_o1(const uint8_t *__restrict__ p, uint64_t n,
                                                const uint2 *__restrict__ tab, const uint8_t *__restrict__ umap,
@@ -432,7 +433,10 @@ __device__ __forceinline__ void encode_warp_o1(const uint8_t *__restrict__ p, ui
             ent[k] = tabat(up * nu + u[k]);
         }
     };
-    uint32_t c1[16], c2[16], wv[16], pwv[16];
+    // c1: symbols of the chunk below the running one; lo1: the round below
+    // c1's lowest (its lane 31 holds the context of c1's lowest lane 0).
+    // Both are loaded one chunk before `entries` reads them.
+    uint32_t c1[16], c2[16], wv[16], pwv[16], lo1, lo2;
     uint2 ent[16], entn[16];
     uint32_t pbits = 0;
 #pragma unroll
@@ -446,12 +450,14 @@ __device__ __forceinline__ void encode_warp_o1(const uint8_t *__restrict__ p, ui
         for (int k = 0; k < 16; k++) c0[k] = c1[k];
 #pragma unroll
         for (int k = 0; k < 16; k++) c1[k] = sym(full - 17 - k);
+        lo1 = sym(full - 33);
         entries(c0, c1[0], ent);
     }
     for (int64_t rt = full - 1; rt >= 0; rt -= 16) {
 #pragma unroll
         for (int k = 0; k < 16; k++) c2[k] = sym(rt - 32 - k);
-        entries(c1, c2[0], entn);
+        lo2 = sym(rt - 48);
+        entries(c1, lo1, entn);
         const bool whole = rt >= 15;
         uint32_t bits = 0;
 #pragma unroll
@@ -468,6 +474,7 @@ __device__ __forceinline__ void encode_warp_o1(const uint8_t *__restrict__ p, ui
             c1[k] = c2[k];
             pwv[k] = wv[k];
         }
+        lo1 = lo2;
     }
 #pragma unroll
     for (int k = 0; k < 16; k++) enc_emit((pbits >> k) & 1u, pwv[k], wptr, lt);

@@ -195,6 +195,9 @@ void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint3
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
                     uint32_t first_polls, cudaStream_t s);
 uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes);
+// Dynamic shared memory with which one CTA of a decode class fills an SM (no
+// other CTA fits beside it); 0 when the class cannot.
+uint32_t dec_exclusive_smem(int cls);
 // CTAs of a decode class that fit on one SM with `smem_bytes` of dynamic
 // shared memory (registers and static shared memory included).
 int dec_blocks_per_sm(int cls, uint32_t smem_bytes);

@@ -34,7 +34,10 @@ struct ParamDef {
 
 const ParamDef kParams[] = {
     {"o1_four_max_streams", &Tuning::o1_four_max_streams, -1, 1 << 30},
+    {"o1_top_latency_pct", &Tuning::o1_top_latency_pct, 0, 100000},
     {"o1_four_top", &Tuning::o1_four_top, -1, 1 << 30},
+    {"o1_small_top", &Tuning::o1_small_top, -1, 1 << 30},
+    {"o1_top_exclusive", &Tuning::o1_top_exclusive, 0, 1},
     {"cta_cap_o0", &Tuning::cta_cap_o0, 1, 64},
     {"cta_cap_o1_small", &Tuning::cta_cap_o1_small, 1, 64},
     {"cta_cap_o1_wide", &Tuning::cta_cap_o1_wide, 1, 64},
@@ -43,6 +46,7 @@ const ParamDef kParams[] = {
     {"dense_edge_small", &Tuning::dense_edge_small, 0, kDenseImageMax},
     {"dense_edge_large", &Tuning::dense_edge_large, 0, kDenseImageMax},
     {"enc_run_ctas_per_sm", &Tuning::enc_run_ctas_per_sm, 1, 64},
+    {"enc_o1_keys", &Tuning::enc_o1_keys, 0, 1},
 };
 
 // Integer value of "key" in a flat JSON object (no nesting inside values).

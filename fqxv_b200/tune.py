@@ -10,9 +10,15 @@ checked byte for byte against the input on every measurement. The
 reference's only run-time choice is its SIMD backend
 (crates/fqxv-rans/src/lib.rs:80-97); these are the GPU's counterparts:
 
-  o1_four_top           the largest this-many wide-alphabet order-1 streams of
-                        a batch decode on the four-warp decoder, in a launch
-                        group of their own
+  o1_top_latency_pct    order-1 streams whose serial decode outlasts this
+                        share of the batch's throughput-bound time decode in
+                        launch groups of their own (wide alphabets on the
+                        four-warp decoder, small ones on the one-warp one)
+  o1_four_top / o1_small_top
+                        at most this many streams in each of those groups
+  o1_top_exclusive      1: those two groups run one CTA per SM alone on it
+  enc_o1_keys           order-1 encode reads per-position table indices stored
+                        by the model kernel (1) or derives them (0)
   o1_four_max_streams   below this many wide-alphabet order-1 streams in a
                         launch group the four-warp decoder (one stream per
                         SM, lower latency per stream) runs them, else the
@@ -41,9 +47,9 @@ from . import workloads as W
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # the library's built-in rules (csrc/rans_ctx.cuh, struct Tuning)
-DEFAULTS = {"o1_four_max_streams": -1, "o1_four_top": -1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
+DEFAULTS = {"o1_four_max_streams": -1, "o1_top_latency_pct": 75, "o1_four_top": -1, "o1_small_top": -1, "o1_top_exclusive": 1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
             "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "dense_edge_small": 40 << 10,
-            "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 16}
+            "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 16, "enc_o1_keys": 1}
 
 
 def _batch(kind: str, nblocks: int, block: int, seed: int):
@@ -138,12 +144,23 @@ def sweep(reps: int = 3) -> dict:
         wide[count] = row
         del b
     meas["gbs_o1_wide_vs_four_by_streams"] = {str(k): {n: round(g, 3) for n, g in v.items()} for k, v in wide.items()}
-    # ... but the rule is chosen on a mix of config 2's stream types and sizes,
-    # where the longest streams bound a launch group rather than its count
-    mix, mspans, _ = W.config2(nblocks=1024, hi=4 << 20, seed=700)
+    # ... but the rules are chosen on config 2's mix of stream types and sizes
+    # (the longest streams bound a launch group rather than its count)
+    # together with two uniform batches, where no stream outlasts the rest:
+    # the score is the geometric mean of the three decode rates
+    mix, mspans, _ = W.config2(seed=700)
     bm = Bench(c, mix, mspans, 2)
-    pick("o1_four_top", (0, sms // 4, sms // 2, sms), lambda: bm.decode_gbs(reps))
-    pick("o1_four_max_streams", (0, sms // 2, sms, 2 * sms, 4 * sms, 1 << 30), lambda: bm.decode_gbs(reps))
+    bu = Bench(c, *_batch("full", 1024, 512 << 10, 710), 1)
+    bf = Bench(c, *_batch("full", 64, 1 << 20, 720), 1)
+
+    def score():
+        g = [bm.decode_gbs(reps), bu.decode_gbs(reps), bf.decode_gbs(reps)]
+        return float(np.exp(np.mean(np.log(g))))
+    pick("o1_top_exclusive", (1, 0), score)
+    pick("o1_top_latency_pct", (25, 50, 75, 100, 150, 100000), score)
+    pick("o1_four_top", (sms // 4, sms // 2, sms), score)
+    pick("o1_small_top", (sms // 4, sms // 2, sms), score)
+    pick("o1_four_max_streams", (0, sms // 2, sms, 2 * sms, 4 * sms, 1 << 30), score)
 
     caps = (1, 2, 4, 8, 16, 32)
     b = Bench(c, *_batch("binned", 1024, 256 << 10, 200), 0)
@@ -180,19 +197,20 @@ def sweep(reps: int = 3) -> dict:
     data, spans, _ = W.config2(nblocks=512, hi=1 << 20, seed=600)
     b = Bench(c, data, spans, 2)
     pick("enc_run_ctas_per_sm", (4, 8, 16, 32), lambda: b.encode_gbs(reps))
+    pick("enc_o1_keys", (1, 0), lambda: b.encode_gbs(reps))
     del b
-    # the whole table against the built-in rules on the mix: decode
-    # parameters fall back to the built-in ones when the table is slower
-    tuned = bm.decode_gbs(reps)
+    # the whole table against the built-in rules on the three batches:
+    # decode parameters fall back to the built-in ones when the table is slower
+    tuned = score()
     for k, v in DEFAULTS.items():
         c.set_param(k, v)
-    builtin = bm.decode_gbs(reps)
-    meas["gbs_mix_decode_table_vs_builtin"] = {"table": round(tuned, 3), "builtin": round(builtin, 3)}
+    builtin = score()
+    meas["gbs_decode_score_table_vs_builtin"] = {"table": round(tuned, 3), "builtin": round(builtin, 3)}
     if builtin > tuned:
         for k in DEFAULTS:
-            if k != "enc_run_ctas_per_sm":
+            if not k.startswith("enc_"):
                 params.pop(k, None)
-    del bm
+    del bm, bu, bf
     c.close()
     return {"device": dev.name, "sm_count": sms, "params": params, "measurements": meas,
             "when": time.strftime("%Y-%m-%d %H:%M:%S")}

@@ -71,6 +71,30 @@ def test_mixed_batch_matches_oracle(codec, orc, mode):
     _roundtrip_check(codec, data, spans, d_out, out_spans)
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+def test_keyless_order1_encode_matches_oracle(codec, orc, mode):
+    """Order-1 encode without the per-position key array (enc_o1_keys = 0):
+    the same bytes as the oracle, small and odd block lengths included."""
+    data, spans, kinds = W.config2(nblocks=48, lo=1, hi=300_000, seed=300 + mode)
+    extra = [np.random.default_rng(s).integers(0, 256, s, dtype=np.uint8) for s in (1, 2, 31, 32, 33, 511, 512, 513, 1025)]
+    data = np.concatenate([data] + extra)
+    lens = [int(x) for x in spans[:, 1]] + [len(e) for e in extra]
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    spans = np.stack([offs, lens], 1).astype(np.uint64)
+    old = codec.get_param("enc_o1_keys")
+    codec.set_param("enc_o1_keys", 0)
+    try:
+        d_out, out_spans, orders = codec.encode_batch(_dev(data), spans, mode)
+    finally:
+        codec.set_param("enc_o1_keys", old)
+    out = d_out.cpu().numpy()
+    ref, roff, rlen = orc.encode_batch(data, spans[:, 0], spans[:, 1], mode)
+    for i in range(len(spans)):
+        got = out[int(out_spans[i, 0]):int(out_spans[i, 0] + out_spans[i, 1])]
+        assert np.array_equal(got, ref[int(roff[i]):int(roff[i] + rlen[i])]), (i, lens[i])
+    _roundtrip_check(codec, data, spans, d_out, out_spans)
+
+
 def test_plain_form_equals_batched(codec):
     data, spans, _ = W.config2(nblocks=24, lo=100, hi=200_000, seed=7)
     d_src = _dev(data)
@@ -258,6 +282,9 @@ def test_launch_shapes_change_no_byte(codec):
         {"o1_four_max_streams": 0, "cta_cap_o1_wide": 1, "enc_run_ctas_per_sm": 4},
         {"o1_four_max_streams": 1 << 30, "cta_cap_o1_four": 1, "dense_edge_small": 0, "dense_edge_large": 0},
         {"cta_cap_o0": 1, "cta_cap_o1_small": 2, "dense_edge_small": 160 << 10, "dense_edge_large": 160 << 10},
+        {"o1_top_exclusive": 0, "o1_four_top": 0, "o1_small_top": 0, "enc_o1_keys": 0},
+        {"o1_top_exclusive": 1, "o1_four_top": 3, "o1_small_top": 5},
+        {"o1_top_exclusive": 1, "o1_four_top": 1 << 20, "o1_small_top": 1 << 20, "enc_o1_keys": 0},
     ]
     defaults = {k: codec.get_param(k) for s in settings for k in s}
     try:

@@ -10,7 +10,10 @@ from conftest import ROOT
 
 KNOWN = {
     "o1_four_max_streams": (-1, 1 << 30),
+    "o1_top_latency_pct": (0, 100000),
     "o1_four_top": (-1, 1 << 30),
+    "o1_small_top": (-1, 1 << 30),
+    "o1_top_exclusive": (0, 1),
     "cta_cap_o0": (1, 64),
     "cta_cap_o1_small": (1, 64),
     "cta_cap_o1_wide": (1, 64),
@@ -19,6 +22,7 @@ KNOWN = {
     "dense_edge_small": (0, 160 * 1024),
     "dense_edge_large": (0, 160 * 1024),
     "enc_run_ctas_per_sm": (1, 64),
+    "enc_o1_keys": (0, 1),
 }
 
 
