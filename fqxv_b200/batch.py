@@ -17,7 +17,8 @@ from . import rans
 
 class StageStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double),
-                ("bytes", ctypes.c_uint64), ("wall_ms", ctypes.c_double)]
+                ("bytes", ctypes.c_uint64), ("wall_ms", ctypes.c_double),
+                ("ctas_per_sm", ctypes.c_uint32), ("smem_bytes", ctypes.c_uint32)]
 
 
 # format.rs:252-266 StreamLoc, as include/fqxv_frame_gpu.h lays it out.
@@ -306,7 +307,9 @@ class Codec:
         rans.raise_for(self._lib.fqxv_rans_ctx_stage_stats(self._h, ctypes.cast(arr, ctypes.c_void_p), 16,
                                                            ctypes.byref(n), 1 if reset else 0))
         return {arr[i].name.decode(): {"launches": int(arr[i].launches), "ms": float(arr[i].ms),
-                                       "bytes": int(arr[i].bytes), "wall_ms": float(arr[i].wall_ms)}
+                                       "bytes": int(arr[i].bytes), "wall_ms": float(arr[i].wall_ms),
+                                       "ctas_per_sm": int(arr[i].ctas_per_sm),
+                                       "smem_bytes": int(arr[i].smem_bytes)}
                 for i in range(n.value)}
 
     def _test_set_wait_polls(self, polls: int) -> None:

@@ -281,20 +281,20 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     {
         // Launch groups: order-0; order-1 small alphabets (one warp per
         // stream, many per SM); order-1 byte columns by table size (the
-        // shared memory of a group is its largest member's), with the
-        // largest of those streams in a group of their own on the four-warp
-        // decoder (`ord` runs largest first); order-1 global.
+        // shared memory of a group is its largest member's); the order-1
+        // streams that bound the batch by their serial time in two groups of
+        // their own (below); order-1 global.
         const DecStream *ps = reinterpret_cast<const DecStream *>(hst);
-        const int64_t four_top = ctx->tune.o1_four_top < 0 ? ctx->sms / 2 : ctx->tune.o1_four_top;
-        const int64_t small_top = ctx->tune.o1_small_top < 0 ? ctx->sms / 2 : ctx->tune.o1_small_top;
+        const int64_t top_max = ctx->tune.o1_top_max < 0 ? ctx->sms / 2 : ctx->tune.o1_top_max;
         // A stream whose serial decode (its rounds one after another) takes
         // longer than o1_top_latency_pct % of the whole batch's throughput-
-        // bound time would finish last however the rest is packed: such
-        // order-1 streams (up to the counts above) form the top groups.
-        // Costs in SM cycles per byte, from B200 measurements: a stream's
-        // latency is cycles per 32-byte round / 32; the batch's throughput
-        // time is the sum over streams of bytes x (SM cycles per byte at the
-        // class's full-GPU rate) / SMs.
+        // bound time would finish last however the rest is packed: the
+        // o1_top_max longest such order-1 streams (by serial time) form the
+        // top groups -- wide alphabets on the four-warp decoder, small ones
+        // on the one-warp decoder. Costs in SM cycles per byte, from B200
+        // measurements: a stream's serial time is cycles per 32-byte round /
+        // 32 per byte; the batch's throughput time is the sum over streams
+        // of bytes x (SM cycles per byte at the class's full-GPU rate) / SMs.
         auto lat_cpb = [](const DecStream &d) {
             return d.cls == kClsO0 ? 5.0 : d.nd <= kShflMaxNd ? 15.0 : d.nd <= kSmallMaxNd ? 18.0 : 19.5;
         };
@@ -305,27 +305,40 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         for (size_t i = 0; i < nb; i++)
             if (ps[i].cls != kClsNone) bulk += (double)ps[i].n * rate_cpb(ps[i]);
         const double top_thr = bulk / ctx->sms * (double)ctx->tune.o1_top_latency_pct / 100.0;
-        int64_t wide_seen = 0, small_seen = 0;
-        auto group_of = [&](const DecStream &d) -> int {
+        std::vector<std::pair<double, uint32_t>> cand;
+        for (size_t i = 0; i < nb; i++) {
+            const DecStream &d = ps[i];
+            const double lat = (double)d.n * lat_cpb(d);
+            if (d.cls == kClsO1Dense && lat > top_thr) cand.emplace_back(lat, (uint32_t)i);
+        }
+        const size_t ntop = std::min<size_t>(cand.size(), (size_t)std::max<int64_t>(top_max, 0));
+        std::partial_sort(cand.begin(), cand.begin() + ntop, cand.end(),
+                          [](const std::pair<double, uint32_t> &a, const std::pair<double, uint32_t> &b) {
+                              return a.first > b.first || (a.first == b.first && a.second < b.second);
+                          });
+        std::vector<uint8_t> is_top(nb, 0);
+        for (size_t k = 0; k < ntop; k++) is_top[cand[k].second] = 1;
+        auto group_of = [&](uint32_t i) -> int {
+            const DecStream &d = ps[i];
             if (d.cls == kClsO0) return 0;
             if (d.cls == kClsO1Global) return kGroups - 1;
             if (d.cls != kClsO1Dense) return -1;
-            const bool top = (double)d.n * lat_cpb(d) > top_thr;
-            if (d.nd <= kSmallMaxNd) return top && small_seen++ < small_top ? kGroupSmallTop : 1;
-            if (top && wide_seen++ < four_top) return kGroupFourTop;
+            if (d.nd <= kSmallMaxNd) return is_top[i] ? kGroupSmallTop : 1;
+            if (is_top[i]) return kGroupFourTop;
             return d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_small   ? 2
                    : d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_large ? 3
                                                                          : 4;
         };
         std::vector<uint32_t> lists[kGroups];
-        uint32_t tmax[kGroups] = {};
+        uint32_t tmax[kGroups] = {}, tmaxp[kGroups] = {};
         uint64_t cbytes[kGroups] = {};
         uint64_t maxn[kGroups] = {};
         for (uint32_t i : ord) {
-            const int g = group_of(ps[i]);
+            const int g = group_of(i);
             if (g < 0) continue;
             lists[g].push_back(i);
             tmax[g] = std::max(tmax[g], ps[i].tbl_bytes);
+            tmaxp[g] = std::max(tmaxp[g], ps[i].tbl_bytes_planes);
             cbytes[g] += ps[i].src_len + ps[i].n;
             maxn[g] = std::max<uint64_t>(maxn[g], ps[i].n);
         }
@@ -338,7 +351,8 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             else if (g == 1 || g == kGroupSmallTop) gcls[g] = kClsO1Small;
             else if (g == kGroupFourTop) gcls[g] = kClsO1Dense;
             else gcls[g] = (int64_t)lists[g].size() < four_max ? kClsO1Dense : kClsO1Wide;
-            smem[g] = dec_smem_bytes(gcls[g], tmax[g]);
+            // the four-warp decoder also stages the bit-plane columns
+            smem[g] = dec_smem_bytes(gcls[g], gcls[g] == kClsO1Dense ? tmaxp[g] : tmax[g]);
             // the groups of largest streams: one CTA per SM, alone on it
             if ((g == kGroupFourTop || g == kGroupSmallTop) && ctx->tune.o1_top_exclusive)
                 smem[g] = std::max(smem[g], dec_exclusive_smem(gcls[g]));
@@ -381,6 +395,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
                                 : cls == kClsO1Wide ? T.cta_cap_o1_wide : cls == kClsO1Dense ? T.cta_cap_o1_four
                                                                                             : T.cta_cap_o1_global;
             per_sm = std::max(1, std::min<int>(per_sm, (int)cap));
+            ctx->timer.shape(stage, per_sm, smem[g]);
             if (persistent) {
                 const int grid = (int)std::min<size_t>(m, (size_t)ctx->sms * per_sm);
                 cudaEvent_t t0 = ctx->timer.begin(as);
@@ -392,7 +407,9 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
                     CK(cudaMemsetAsync(queue + 4 * g, 0, 4, as));
                     cudaEvent_t t0 = ctx->timer.begin(as);
                     launch_dec_run(cls, d_src, dS, dl + base[g] + j, 1, dT, d_dst, queue + 4 * g, 1,
-                                   dec_smem_bytes(cls, ps[lists[g][j]].tbl_bytes), ctx->first_polls, as);
+                                   dec_smem_bytes(cls, cls == kClsO1Dense ? ps[lists[g][j]].tbl_bytes_planes
+                                                                          : ps[lists[g][j]].tbl_bytes),
+                                   ctx->first_polls, as);
                     ctx->timer.end(stage, t0, as);
                 }
             }
@@ -724,6 +741,8 @@ int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int
         out[k].ms = ctx->timer.ms[i];
         out[k].bytes = ctx->timer.bytes[i];
         out[k].wall_ms = ctx->timer.wall_ms[i];
+        out[k].ctas_per_sm = ctx->timer.ctas_per_sm[i];
+        out[k].smem_bytes = ctx->timer.smem_bytes[i];
     }
     *n = k;
     if (reset) {
@@ -732,6 +751,8 @@ int fqxv_rans_ctx_stage_stats(fqxv_rans_ctx *ctx, fqxv_rans_stage_stat *out, int
             ctx->timer.ms[i] = 0.0;
             ctx->timer.wall_ms[i] = 0.0;
             ctx->timer.bytes[i] = 0;
+            ctx->timer.ctas_per_sm[i] = 0;
+            ctx->timer.smem_bytes[i] = 0;
         }
     }
     return FQXV_RANS_OK;

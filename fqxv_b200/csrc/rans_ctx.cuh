@@ -3,6 +3,7 @@
 // fqxv_rans_ctx. Nothing here is part of the public ABI.
 #pragma once
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -99,14 +100,12 @@ struct Tuning {
     // (several per SM). -1: the SM count.
     int64_t o1_four_max_streams = -1;
     // Order-1 streams whose serial decode alone outlasts o1_top_latency_pct %
-    // of the batch's throughput-bound time form launch groups of their own
-    // (the batch lasts at least as long as its longest serial chain): wide
-    // alphabets on the four-warp decoder, at most o1_four_top streams, small
-    // alphabets on the one-warp decoder, at most o1_small_top. -1: half the
-    // SM count.
+    // of the batch's throughput-bound time -- the o1_top_max longest of them
+    // -- form launch groups of their own (the batch lasts at least as long as
+    // its longest serial chain): wide alphabets on the four-warp decoder,
+    // small ones on the one-warp decoder. o1_top_max -1: half the SM count.
     int64_t o1_top_latency_pct = 75;
-    int64_t o1_four_top = -1;
-    int64_t o1_small_top = -1;
+    int64_t o1_top_max = -1;
     // 1: those two groups run one CTA per SM with no other CTA beside it
     // (their CTAs claim the SM's shared memory), so their serial chains are
     // not slowed by the rest of the batch; 0: they share.
@@ -149,6 +148,14 @@ struct StageTimer {
     double wall_ms[kStages] = {};
     uint64_t launches[kStages] = {};
     uint64_t bytes[kStages] = {};   // algorithmic bytes moved by the stage's launches
+    // launch shape, largest over the stage's launches: CTAs per SM and
+    // dynamic shared memory per CTA
+    uint32_t ctas_per_sm[kStages] = {};
+    uint32_t smem_bytes[kStages] = {};
+    void shape(int stage, int per_sm, uint32_t smem) {
+        ctas_per_sm[stage] = std::max(ctas_per_sm[stage], (uint32_t)std::max(per_sm, 0));
+        smem_bytes[stage] = std::max(smem_bytes[stage], smem);
+    }
     cudaEvent_t get() {
         if (!pool.empty()) {
             cudaEvent_t e = pool.back();

@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(kParseThreads)
             S.nd = 0;
             S.start = 0;
             S.tbl_bytes = 0;
+            S.tbl_bytes_planes = 0;
         }
         if (status != FQXV_RANS_OK || n == 0) {
             if (tid == 0) S.status = status;
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(kParseThreads)
                 if (tid == 0) {
                     S.cls = kClsO0;
                     S.tbl_bytes = 16384;
+                    S.tbl_bytes_planes = 16384;
                 }
             }
         } else if (L < kHdr + kO1Bitmap) {
@@ -299,6 +301,23 @@ __global__ void __launch_bounds__(kParseThreads)
                         }
                     }
                     __syncthreads();
+                    // bit planes of every column, when they fit beside the image
+                    const bool planes = dense_planes(nd) &&
+                                        dense_table_bytes(nd, ncol) + kPlaneStride * ncol <= kDenseImageMax;
+                    if (planes) {
+                        uint32_t *PL = reinterpret_cast<uint32_t *>(T + dense_table_bytes(nd, ncol));
+                        for (uint32_t j = warp; j < ncol; j += kParseThreads / 32) {
+                            const uint32_t v = COL[j * cs + lane];
+                            uint32_t w = 0;
+#pragma unroll
+                            for (int b = 0; b < 5; b++) {
+                                const uint32_t pl = __ballot_sync(0xffffffffu, (v >> b) & 1u);
+                                if (lane == b) w = __funnelshift_l(pl, pl, b);
+                            }
+                            if (lane < 8) PL[j * (kPlaneStride / 4) + lane] = w;
+                        }
+                        __syncthreads();
+                    }
                     if (packed) {
                         // 16 entries of a 16-byte column -> 16 nibbles
                         uint64_t *PK = reinterpret_cast<uint64_t *>(T + dense_col_off(nd));
@@ -314,6 +333,7 @@ __global__ void __launch_bounds__(kParseThreads)
                         S.nd = nd;
                         S.start = dmap[0] != 0xff ? dmap[0] : dead;
                         S.tbl_bytes = dense_table_bytes(nd, ncol);
+                        S.tbl_bytes_planes = S.tbl_bytes + (planes ? kPlaneStride * ncol : 0u);
                     }
                 } else {
                     if (tid < 256) T[kDecCtxMap + tid] = ctxmap[tid];
@@ -924,6 +944,97 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
     return o1_rounds(S, R, out, lt, ByteCols{I.M}, I.FC, I.DS, I.stride, dead, warp == 0, x, resolve);
 }
 
+// Four-warp decode of a stream with bit-plane columns (kSmallMaxNd < |D| <=
+// kPlaneMaxNd). Warp w >= 1 runs segment w for every incoming context, lane
+// c from context c, and lane 31 of every warp runs segment 0 from the known
+// context, so each warp has the first segment's row in registers. A chain
+// step looks its next context up in the column's five bit planes (loaded
+// into registers once per round): plane p rotated right by the context puts
+// the entry's bit p at bit p, and four bit selects merge the five. Rows are
+// (segment, context) pairs, 32 per segment; row (s, 31) is the DEAD row
+// when |D| = 31 (the DEAD context is then 31, whose lane runs segment 0)
+// and is never reached otherwise. The round is then resolved as in
+// o1d_stream: three dependent row loads after the barrier.
+__device__ __forceinline__ int o1p_stream(DecStream &S, const uint8_t *__restrict__ sm, WordRing &R,
+                                          uint4 (*__restrict__ rows)[kOutRows + 1], uint8_t *__restrict__ out,
+                                          uint32_t lt) {
+    static_assert(4 * 32 <= kOutRows + 1, "row array holds four segments of 32 rows");
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nd = S.nd;
+    const DenseImage I(sm, nd);
+    const uint32_t dead = I.dead;
+    const uint8_t *PL = sm + S.tbl_bytes;
+    const uint32_t myseg = lane == 31 ? 0u : (uint32_t)warp;
+    const bool writer = warp >= 1 && lane < 31;
+    const uint32_t nbase = 32u * (myseg + 1u);  // row of context 0 in the next segment
+    const uint32_t deadw = 0x01010101u * dead;
+    if (tid < 6) {
+        const uint32_t sg = 1u + (uint32_t)(tid % 3);
+        rows[tid / 3][32u * sg + 31u] = make_uint4(deadw, deadw, 16u * (32u * (sg + 1u) + 31u), 0u);
+    }
+    uint32_t din = (uint32_t)S.start;
+    const int seg = lane >> 3, pos = lane & 7;
+    const uint32_t shd = 24u - 8u * (uint32_t)(pos & 3);
+    const uint32_t shc = 24u - 8u * (uint32_t)((pos + 3) & 3);
+    uint32_t buf = 0;
+
+    auto resolve = [&](uint32_t, uint32_t cb, uint32_t &d, uint32_t &ctx) {
+        uint32_t q[8][5];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t off = __shfl_sync(0xffffffffu, cb, 8 * myseg + k);
+            const uint4 a = *reinterpret_cast<const uint4 *>(PL + off);
+            q[k][0] = a.x;
+            q[k][1] = a.y;
+            q[k][2] = a.z;
+            q[k][3] = a.w;
+            q[k][4] = *reinterpret_cast<const uint32_t *>(PL + off + 16);
+        }
+        uint32_t dd = lane == 31 ? din : (uint32_t)lane;
+        uint32_t hi = 0, lo = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const uint32_t t0 = __funnelshift_r(q[k][0], q[k][0], dd);
+            const uint32_t t1 = __funnelshift_r(q[k][1], q[k][1], dd);
+            const uint32_t t2 = __funnelshift_r(q[k][2], q[k][2], dd);
+            const uint32_t t3 = __funnelshift_r(q[k][3], q[k][3], dd);
+            const uint32_t t4 = __funnelshift_r(q[k][4], q[k][4], dd);
+            const uint32_t a = (t0 & 1u) | (t1 & ~1u);
+            const uint32_t b = (t2 & 7u) | (t3 & ~7u);
+            const uint32_t c = (a & 3u) | (b & ~3u);
+            // bits above 4 are left over from the planes: a funnel shift
+            // uses its amount mod 32, and the row keeps the clean value
+            dd = (c & 15u) | (t4 & ~15u);
+            if (k < 4) hi = (hi << 8) | (dd & 31u);
+            else lo = (lo << 8) | (dd & 31u);
+        }
+        const uint32_t nx = 16u * (nbase + (dd & 31u));
+        uint4 *rb = rows[buf];
+        if (writer) rb[32 * warp + lane] = make_uint4(hi, lo, nx, 0u);
+        uint4 r0;
+        r0.x = __shfl_sync(0xffffffffu, hi, 31);
+        r0.y = __shfl_sync(0xffffffffu, lo, 31);
+        r0.z = __shfl_sync(0xffffffffu, nx, 31);
+        named_bar(1);
+        const uint8_t *rbb = reinterpret_cast<const uint8_t *>(rb);
+        const uint4 r1 = *reinterpret_cast<const uint4 *>(rbb + r0.z);
+        const uint4 r2 = *reinterpret_cast<const uint4 *>(rbb + r1.z);
+        const uint32_t rx = seg == 0 ? r0.x : seg == 1 ? r1.x : r2.x;
+        const uint32_t ry = seg == 0 ? r0.y : seg == 1 ? r1.y : r2.y;
+        const uint32_t ine = seg == 0 ? din : seg == 1 ? (r0.y & 0xffu) : (r1.y & 0xffu);
+        const uint4 r3 = *reinterpret_cast<const uint4 *>(rbb + r2.z);
+        const uint32_t row_x = seg == 3 ? r3.x : rx;
+        const uint32_t row_y = seg == 3 ? r3.y : ry;
+        const uint32_t in = seg == 3 ? (r2.y & 0xffu) : ine;
+        d = ((pos < 4 ? row_x : row_y) >> shd) & 0xffu;
+        ctx = pos == 0 ? in : ((pos <= 4 ? row_x : row_y) >> shc) & 0xffu;
+        din = r3.y & 0xffu;
+        buf ^= 1u;
+    };
+
+    return o1_rounds(S, R, out, lt, ByteCols{I.M}, I.FC, I.DS, I.stride, dead, warp == 0, S.states[lane], resolve);
+}
+
 __global__ void __launch_bounds__(kO1Threads, 1)
     dec_o1d_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
@@ -949,7 +1060,7 @@ __global__ void __launch_bounds__(kO1Threads, 1)
         if (warp == 0) {
             bool ok = false;
             if (!s_stuck) {
-                st.issue(sm, tbl + S.tbl_off, S.tbl_bytes);
+                st.issue(sm, tbl + S.tbl_off, S.tbl_bytes_planes);
                 ok = st.wait(first_polls);
                 if (!ok && !st.drain() && lane == 0) s_stuck = 1;
             }
@@ -963,8 +1074,9 @@ __global__ void __launch_bounds__(kO1Threads, 1)
         if (!s_ok) continue;
         uint8_t *out = dst + S.dst_off;
         const int tpl = (3 * S.nd + kO1Workers - 1) / kO1Workers;
-        const int status = tpl <= 1 ? o1d_stream<1>(S, sm, R, s_rows, out, lt)
-                                    : o1d_stream<2>(S, sm, R, s_rows, out, lt);
+        const int status = S.tbl_bytes_planes > S.tbl_bytes ? o1p_stream(S, sm, R, s_rows, out, lt)
+                           : tpl <= 1                       ? o1d_stream<1>(S, sm, R, s_rows, out, lt)
+                                                            : o1d_stream<2>(S, sm, R, s_rows, out, lt);
         if (tid == 0) S.status = status;
         __syncthreads();
     }
@@ -1365,6 +1477,16 @@ static void ensure_dec_attrs() {
                          (int)std::max(dec_smem_bytes(kClsO1Small, kDenseImageMax), dec_exclusive_smem(kClsO1Small)));
     cudaFuncSetAttribute(dec_o1w_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)dec_smem_bytes(kClsO1Wide, kDenseImageMax));
+    // Kernels whose tables live in shared memory take the largest shared-
+    // memory share of the SM's L1, so as many streams as fit run per SM (the
+    // global-table decoder keeps its L1 for the tables it reads through it).
+    cudaFuncSetAttribute(dec_o0_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(dec_o1d_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(dec_o1w_kernel<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(dec_o1w_kernel<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaGetLastError();
     g_attr_done[dev] = true;
 }
 

@@ -747,6 +747,10 @@ void launch_enc_run(const uint8_t *src, EncBlock *blocks, const EncJob *jobs, in
         if (dev >= 0 && dev < 256 && !done[dev]) {
             cudaFuncSetAttribute(enc_run_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kEncWarpsPerCta * kEncO1TabBytes));
+            // three CTAs per SM (the register limit) need ~225 KB of shared memory
+            cudaFuncSetAttribute(enc_run_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+            cudaGetLastError();
             done[dev] = true;
         }
     }

@@ -88,6 +88,8 @@ struct DecStream {
     int32_t nd;                  // dense format: |D| (symbols and contexts), DEAD = nd
     int32_t start;               // dense format: index of context 0 (DEAD when absent)
     uint32_t tbl_bytes;          // bytes of the table image staged into shared memory
+    uint32_t tbl_bytes_planes;   // dense format with bit-plane columns: image + planes
+                                 // (the four-warp decoder stages these); else tbl_bytes
     uint32_t states[kStates];
 };
 
@@ -143,6 +145,16 @@ __host__ __device__ inline uint32_t dense_table_bytes(int nd, uint32_t ncol) {
     return dense_packed(nd) ? dense_col_off(nd) + (8 * ncol + 15) / 16 * 16
                             : dense_col_off(nd) + ncol * dense_col_stride(nd);
 }
+// Bit-plane columns, kSmallMaxNd < |D| <= kPlaneMaxNd: after the byte
+// columns, column j's entries as five u32 planes at j * 32 (plane p, bit c =
+// bit p of the entry of context c, rotated left by p; three words of
+// padding), so that a chain step is five funnel shifts and four bit selects
+// in registers instead of a shared-memory load. The planes offset is
+// dense_table_bytes, and column j's planes sit at the byte offset of its byte
+// column (the byte stride is 32 for these |D|).
+constexpr int kPlaneMaxNd = 31;
+constexpr uint32_t kPlaneStride = 32;
+__host__ __device__ inline bool dense_planes(int nd) { return nd > kSmallMaxNd && nd <= kPlaneMaxNd; }
 // Bytes the parse needs in the arena while building the image: the packed
 // form is built from byte columns placed after it.
 __host__ __device__ inline uint32_t dense_build_bytes(int nd, uint32_t ncol) {

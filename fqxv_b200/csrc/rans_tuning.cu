@@ -35,8 +35,7 @@ struct ParamDef {
 const ParamDef kParams[] = {
     {"o1_four_max_streams", &Tuning::o1_four_max_streams, -1, 1 << 30},
     {"o1_top_latency_pct", &Tuning::o1_top_latency_pct, 0, 100000},
-    {"o1_four_top", &Tuning::o1_four_top, -1, 1 << 30},
-    {"o1_small_top", &Tuning::o1_small_top, -1, 1 << 30},
+    {"o1_top_max", &Tuning::o1_top_max, -1, 1 << 30},
     {"o1_top_exclusive", &Tuning::o1_top_exclusive, 0, 1},
     {"cta_cap_o0", &Tuning::cta_cap_o0, 1, 64},
     {"cta_cap_o1_small", &Tuning::cta_cap_o1_small, 1, 64},

@@ -14,8 +14,8 @@ reference's only run-time choice is its SIMD backend
                         share of the batch's throughput-bound time decode in
                         launch groups of their own (wide alphabets on the
                         four-warp decoder, small ones on the one-warp one)
-  o1_four_top / o1_small_top
-                        at most this many streams in each of those groups
+  o1_top_max            at most this many streams (the longest) in those
+                        groups
   o1_top_exclusive      1: those two groups run one CTA per SM alone on it
   enc_o1_keys           order-1 encode reads per-position table indices stored
                         by the model kernel (1) or derives them (0)
@@ -47,7 +47,7 @@ from . import workloads as W
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # the library's built-in rules (csrc/rans_ctx.cuh, struct Tuning)
-DEFAULTS = {"o1_four_max_streams": -1, "o1_top_latency_pct": 75, "o1_four_top": -1, "o1_small_top": -1, "o1_top_exclusive": 1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
+DEFAULTS = {"o1_four_max_streams": -1, "o1_top_latency_pct": 75, "o1_top_max": -1, "o1_top_exclusive": 1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
             "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "dense_edge_small": 40 << 10,
             "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 16, "enc_o1_keys": 1}
 
@@ -158,18 +158,19 @@ def sweep(reps: int = 3) -> dict:
         return float(np.exp(np.mean(np.log(g))))
     pick("o1_top_exclusive", (1, 0), score)
     pick("o1_top_latency_pct", (25, 50, 75, 100, 150, 100000), score)
-    pick("o1_four_top", (sms // 4, sms // 2, sms), score)
-    pick("o1_small_top", (sms // 4, sms // 2, sms), score)
+    pick("o1_top_max", (sms // 4, sms // 2, 3 * sms // 4, sms), score)
     pick("o1_four_max_streams", (0, sms // 2, sms, 2 * sms, 4 * sms, 1 << 30), score)
 
-    caps = (1, 2, 4, 8, 16, 32)
-    b = Bench(c, *_batch("binned", 1024, 256 << 10, 200), 0)
+    # CTAs per SM on batches of the peak-throughput shape (2048 x 512 KiB):
+    # enough streams that every cap fills the GPU several times over
+    caps = (1, 2, 3, 4, 5, 6, 8, 16, 32)
+    b = Bench(c, *_batch("binned", 2048, 512 << 10, 200), 0)
     pick("cta_cap_o0", caps, lambda: b.decode_gbs(reps))
     del b
-    b = Bench(c, *_batch("binned", 1024, 256 << 10, 300), 1)
+    b = Bench(c, *_batch("binned", 2048, 512 << 10, 300), 1)
     pick("cta_cap_o1_small", caps, lambda: b.decode_gbs(reps))
     del b
-    b = Bench(c, *_batch("full", 1024, 256 << 10, 400), 1)
+    b = Bench(c, *_batch("full", 2048, 512 << 10, 400), 1)
     pick("cta_cap_o1_wide", caps, lambda: b.decode_gbs(reps))
     del b
     # dense group edges on a mix of wide-alphabet types (name tokens, full-range, long-read quality)

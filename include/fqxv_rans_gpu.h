@@ -243,8 +243,7 @@ int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int order, uint8_t 
  * the tuning table of
  * the device when one is found (FQXV_RANS_TUNING, else tuning/<device>.json
  * beside the package directory of the library), else from the built-in
- * rules. Names: o1_four_max_streams, o1_top_latency_pct, o1_four_top, o1_small_top,
- * o1_top_exclusive,
+ * rules. Names: o1_four_max_streams, o1_top_latency_pct, o1_top_max, o1_top_exclusive,
  * cta_cap_o0, cta_cap_o1_small,
  * cta_cap_o1_wide, cta_cap_o1_four, cta_cap_o1_global, dense_edge_small,
  * dense_edge_large, enc_run_ctas_per_sm, enc_o1_keys. Unknown names and out-of-range
@@ -267,7 +266,9 @@ typedef struct fqxv_rans_stage_stat {
     uint64_t launches;
     double ms;
     uint64_t bytes;   /* algorithmic bytes (input read + output written) of those launches */
-    double wall_ms;
+    double wall_ms;       /* first launch start to last launch end, per call, summed */
+    uint32_t ctas_per_sm; /* decode stages: CTAs per SM of the largest launch shape */
+    uint32_t smem_bytes;  /* decode stages: dynamic shared memory per CTA, largest */
 } fqxv_rans_stage_stat;
 
 int fqxv_rans_ctx_set_profiling(fqxv_rans_ctx *ctx, int on);

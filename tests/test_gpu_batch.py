@@ -282,9 +282,9 @@ def test_launch_shapes_change_no_byte(codec):
         {"o1_four_max_streams": 0, "cta_cap_o1_wide": 1, "enc_run_ctas_per_sm": 4},
         {"o1_four_max_streams": 1 << 30, "cta_cap_o1_four": 1, "dense_edge_small": 0, "dense_edge_large": 0},
         {"cta_cap_o0": 1, "cta_cap_o1_small": 2, "dense_edge_small": 160 << 10, "dense_edge_large": 160 << 10},
-        {"o1_top_exclusive": 0, "o1_four_top": 0, "o1_small_top": 0, "enc_o1_keys": 0},
-        {"o1_top_exclusive": 1, "o1_four_top": 3, "o1_small_top": 5},
-        {"o1_top_exclusive": 1, "o1_four_top": 1 << 20, "o1_small_top": 1 << 20, "enc_o1_keys": 0},
+        {"o1_top_exclusive": 0, "o1_top_max": 0, "enc_o1_keys": 0},
+        {"o1_top_exclusive": 1, "o1_top_max": 5, "o1_top_latency_pct": 0},
+        {"o1_top_exclusive": 1, "o1_top_max": 1 << 20, "o1_top_latency_pct": 0, "enc_o1_keys": 0},
     ]
     defaults = {k: codec.get_param(k) for s in settings for k in s}
     try:

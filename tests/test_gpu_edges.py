@@ -127,7 +127,7 @@ def _dense_size(data):
     return len(set(np.unique(prev).tolist()) | set(np.unique(data).tolist()))
 
 
-CLASS_EDGES = [2, 5, 9, 10, 11, 12, 15, 16, 24, 31, 32, 33, 41, 46, 47, 48, 49, 64, 100, 256]
+CLASS_EDGES = [2, 5, 9, 10, 11, 12, 15, 16, 17, 24, 30, 31, 32, 33, 41, 46, 47, 48, 49, 64, 100, 256]
 
 
 @pytest.mark.parametrize("nd", CLASS_EDGES)

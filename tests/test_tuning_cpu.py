@@ -11,8 +11,7 @@ from conftest import ROOT
 KNOWN = {
     "o1_four_max_streams": (-1, 1 << 30),
     "o1_top_latency_pct": (0, 100000),
-    "o1_four_top": (-1, 1 << 30),
-    "o1_small_top": (-1, 1 << 30),
+    "o1_top_max": (-1, 1 << 30),
     "o1_top_exclusive": (0, 1),
     "cta_cap_o0": (1, 64),
     "cta_cap_o1_small": (1, 64),
