@@ -1297,8 +1297,10 @@ def main() -> None:
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": gpu_launches,
-            "stages": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "wall_ms": round(v["wall_ms"], 4),
-                           "bytes": v["bytes"]}
+            "stages": {k: dict({"launches": v["launches"], "ms": round(v["ms"], 4), "wall_ms": round(v["wall_ms"], 4),
+                                "bytes": v["bytes"]},
+                               **({"ctas_per_sm": v["ctas_per_sm"], "smem_bytes": v["smem_bytes"]}
+                                  if v.get("ctas_per_sm") else {}))
                        for k, v in stages.items() if v["launches"]},
             "clocks": clocks,
         }

@@ -224,7 +224,7 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
 
 int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_span *blocks, size_t nb,
                       uint64_t max_len, uint8_t *d_dst, const fqxv_rans_span *out_spans, uint64_t *out_lens,
-                      int32_t *status, int persistent) {
+                      int32_t *status, int persistent, uint8_t *mirror = nullptr) {
     if (nb == 0) return FQXV_RANS_OK;
     if (nb > (1u << 30)) return FQXV_RANS_E_TOO_LARGE;
     NvtxRange range("fqxv.decode_batch");
@@ -325,9 +325,9 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             if (d.cls != kClsO1Dense) return -1;
             if (d.nd <= kSmallMaxNd) return is_top[i] ? kGroupSmallTop : 1;
             if (is_top[i]) return kGroupFourTop;
-            return d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_small   ? 2
-                   : d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_large ? 3
-                                                                         : 4;
+            return d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_small   ? kGroupDense0
+                   : d.tbl_bytes <= (uint64_t)ctx->tune.dense_edge_large ? kGroupDense0 + 1
+                                                                         : kGroupDense0 + 2;
         };
         std::vector<uint32_t> lists[kGroups];
         uint32_t tmax[kGroups] = {}, tmaxp[kGroups] = {};
@@ -400,7 +400,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
                 const int grid = (int)std::min<size_t>(m, (size_t)ctx->sms * per_sm);
                 cudaEvent_t t0 = ctx->timer.begin(as);
                 launch_dec_run(cls, d_src, dS, dl + base[g], (int)m, dT, d_dst, queue + 4 * g, grid, smem[g],
-                               ctx->first_polls, as);
+                               ctx->first_polls, mirror, as);
                 ctx->timer.end(stage, t0, as);
             } else {
                 for (size_t j = 0; j < m; j++) {
@@ -409,7 +409,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
                     launch_dec_run(cls, d_src, dS, dl + base[g] + j, 1, dT, d_dst, queue + 4 * g, 1,
                                    dec_smem_bytes(cls, cls == kClsO1Dense ? ps[lists[g][j]].tbl_bytes_planes
                                                                           : ps[lists[g][j]].tbl_bytes),
-                                   ctx->first_polls, as);
+                                   ctx->first_polls, mirror, as);
                     ctx->timer.end(stage, t0, as);
                 }
             }
@@ -766,9 +766,14 @@ namespace {
 // where this batch's streams go in h_dst (it may wait for an earlier chunk)
 // -- copied out. Offsets of out_spans are local to the batch on entry to
 // `place` and final on return.
-template <class Place>
+// `gate(s, before)` runs on the batch's stream right before (before = true)
+// and after its input copy is issued, so that chunks can order their copies.
+struct NoGate {
+    void operator()(cudaStream_t, bool) const {}
+};
+template <class Place, class Gate = NoGate>
 int encode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_span *blocks, size_t nblocks,
-                    int order, fqxv_rans_span *out_spans, int32_t *out_orders, Place &&place) {
+                    int order, fqxv_rans_span *out_spans, int32_t *out_orders, Place &&place, Gate &&gate = Gate()) {
     DeviceGuard dg(ctx->device);
     cudaStream_t s = ctx->stream;
     uint64_t end = 0;
@@ -776,7 +781,10 @@ int encode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
     const uint64_t bound = fqxv_rans_encode_batch_bound(blocks, nblocks, order);
     CK(ctx->io_in.ensure(std::max<uint64_t>(end, 16), s));
     CK(ctx->io_out.ensure(std::max<uint64_t>(bound, 16), s));
-    CK(cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s));
+    gate(s, true);
+    const cudaError_t ce = cudaMemcpyAsync(ctx->io_in.p, h_src, end, cudaMemcpyHostToDevice, s);
+    gate(s, false);
+    CK(ce);
     int st = encode_batch_impl(ctx, ctx->io_in.as<uint8_t>(), blocks, nblocks, order, ctx->io_out.as<uint8_t>(),
                                bound, out_spans, out_orders, 1);
     const uint64_t total = st ? 0 : out_spans[nblocks - 1].offset + out_spans[nblocks - 1].length;
@@ -790,14 +798,13 @@ int encode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
 }
 
 // Host-buffer batches of at least kPipeMinBytes are cut into up to
-// kPipeChunks chunks of consecutive blocks, each coded by its own
+// `host_chunks` chunks of consecutive blocks, each coded by its own
 // sub-context on its own host thread: one chunk's copies overlap the other
 // chunks' kernels, and chunks of equal blocks run side by side on the GPU.
 constexpr uint64_t kPipeMinBytes = 32ull << 20;
-constexpr int kPipeChunks = 4;
 
 // [first, last) block ranges of roughly equal bytes
-std::vector<std::pair<size_t, size_t>> pipe_chunks(const fqxv_rans_span *blocks, size_t n) {
+std::vector<std::pair<size_t, size_t>> pipe_chunks(const fqxv_rans_span *blocks, size_t n, int64_t nchunks) {
     std::vector<std::pair<size_t, size_t>> out;
     uint64_t total = 0;
     for (size_t i = 0; i < n; i++) total += blocks[i].length;
@@ -805,7 +812,7 @@ std::vector<std::pair<size_t, size_t>> pipe_chunks(const fqxv_rans_span *blocks,
         out.emplace_back(0, n);
         return out;
     }
-    const int k = (int)std::min<size_t>(kPipeChunks, n);
+    const int k = (int)std::min<size_t>((size_t)std::max<int64_t>(nchunks, 1), n);
     size_t b = 0;
     uint64_t acc = 0;
     for (int c = 0; c < k && b < n; c++) {
@@ -856,7 +863,7 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
     if (nblocks == 0) return FQXV_RANS_OK;
     NvtxRange range("fqxv.encode_batch_host");
     std::lock_guard<std::mutex> g(ctx->mu);
-    const auto chunks = pipe_chunks(blocks, nblocks);
+    const auto chunks = pipe_chunks(blocks, nblocks, ctx->tune.host_chunks);
     if (chunks.size() == 1) {
         return encode_host_one(ctx, h_src, blocks, nblocks, order, out_spans, out_orders,
                                [&](int st, uint64_t total, uint8_t *&dst) -> int {
@@ -877,6 +884,18 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
     std::vector<int> ready(k + 1, 0), sts(k, FQXV_RANS_OK);
     ready[0] = 1;
     bool failed = false;
+    // The chunks' input copies go one after another in chunk order (each
+    // chunk's copy waits on the previous one's), so the first chunk's
+    // encode starts after a quarter of the input has crossed the host link
+    // instead of after all of it.
+    std::vector<cudaEvent_t> copied(k, nullptr);
+    for (size_t c = 0; c < k; c++)
+        if (cudaEventCreateWithFlags(&copied[c], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            copied[c] = nullptr;
+        }
+    std::vector<int> issued(k + 1, 0);
+    issued[0] = 1;
     std::vector<std::thread> th;
     for (size_t c = 0; c < k; c++) {
         th.emplace_back([&, c] {
@@ -902,6 +921,17 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
                                          ready[c + 1] = 1;
                                          pcv.notify_all();
                                          return r;
+                                     },
+                                     [&, c](cudaStream_t s, bool before) {
+                                         std::unique_lock<std::mutex> lk(pm);
+                                         if (before) {
+                                             pcv.wait(lk, [&] { return issued[c] != 0; });
+                                             if (c > 0 && copied[c - 1]) cudaStreamWaitEvent(s, copied[c - 1], 0);
+                                         } else {
+                                             if (copied[c]) cudaEventRecord(copied[c], s);
+                                             issued[c + 1] = 1;
+                                             pcv.notify_all();
+                                         }
                                      });
             // a chunk that stopped before placing its output (a failed copy
             // or allocation) still releases the chunks after it
@@ -909,11 +939,14 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
             if (!ready[c + 1]) {
                 failed = true;
                 ready[c + 1] = 1;
-                pcv.notify_all();
             }
+            issued[c + 1] = 1;
+            pcv.notify_all();
         });
     }
     for (auto &t : th) t.join();
+    for (cudaEvent_t e : copied)
+        if (e) cudaEventDestroy(e);
     // the first failing chunk in block order decides (a later chunk that only
     // stopped because an earlier one failed reports that one's status)
     for (size_t c = 0; c < k; c++)
@@ -938,17 +971,12 @@ int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
     }
     // The compressed input of a batch of fewer than kZeroCopyMinStreams
     // streams is staged by one copy, issued first (the decoders' word reads
-    // are latency-sensitive); a pinned (mapped) destination of a large batch
-    // is written by the kernels in place over the host link, so the output
-    // transfer overlaps the decode instead of following it (stores are
-    // posted, nothing waits on them). Other destinations are staged.
-    // In place only while the decode's output rate stays under what the host
-    // link takes as small stores (about 30 GB/s was still faster in place
-    // than a copy afterwards, measured on B200); faster batches are
-    // better served by one bulk copy afterwards. The decode time is
-    // estimated from the stream headers: the largest stream's serial rounds
-    // (about 320 ns per 32 bytes for order-1, 80 ns for order-0 on B200) or
-    // the whole batch at the batched rates (about 15 and 300 GB/s).
+    // are latency-sensitive). A pinned (mapped) destination of a large batch
+    // is mirrored: the kernels decode into device memory and the CTA that
+    // finished a stream copies it to the destination in 16-byte stores
+    // while other streams still decode, so the output transfer overlaps the
+    // decode instead of following it. Other destinations are staged and
+    // copied once the batch is done.
     const uint8_t *d_in = nullptr;
     auto stage_input = [&]() -> cudaError_t {
         cudaError_t e = ctx->io_in.ensure(std::max<uint64_t>(end, 16), s);
@@ -956,42 +984,52 @@ int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
         d_in = ctx->io_in.as<uint8_t>();
         return e;
     };
-    if (nblocks < kZeroCopyMinStreams) CK(stage_input());
-    double t_lat = 0.0, b0 = 0.0, b1 = 0.0;
-    for (size_t i = 0; i < nblocks; i++) {
-        if (blocks[i].length < kHdr) continue;
-        const uint8_t *h = h_src + blocks[i].offset;
-        uint64_t n = 0;
-        for (int k = 0; k < 8; k++) n |= (uint64_t)h[1 + k] << (8 * k);
-        if (n > out_spans[i].length) continue;
-        const bool o1 = h[0] == 1;
-        t_lat = std::max(t_lat, (double)(n / 32) * (o1 ? 320e-9 : 80e-9));
-        (o1 ? b1 : b0) += (double)n;
-    }
-    const double t_est = std::max(t_lat, b1 / 15e9 + b0 / 300e9);
-    const bool in_place = oend >= kZeroCopyMinBytes && t_est > 0.0 && (double)oend / t_est < 40e9;
-    uint8_t *d_out = in_place ? static_cast<uint8_t *>(mapped_device_ptr(h_dst)) : nullptr;
+    const int64_t in_place = ctx->tune.host_in_place;
+    if (in_place == 0 || (in_place < 0 && nblocks < kZeroCopyMinStreams)) CK(stage_input());
+    uint8_t *mirror = oend >= kZeroCopyMinBytes && ctx->tune.host_out_mirror
+                          ? static_cast<uint8_t *>(mapped_device_ptr(h_dst))
+                          : nullptr;
     // A slow batch of hundreds of streams also reads its pinned input in
     // place: each stream's words are fetched 16 bytes a lane, segments ahead
     // of use, at a small share of the link, and the decode starts without
     // waiting for a copy. Measured on B200: 4103 mixed streams (4 KiB to
     // 4 MiB) e2e 17.2 -> 21.2 GB/s, but chunks of 16 x 1 MiB order-1 streams
     // 4.63 -> 4.36, so smaller batches (and single serving requests) keep
-    // the staged copy, issued before the estimate above.
-    if (!d_in && d_out) d_in = static_cast<const uint8_t *>(mapped_device_ptr(h_src));
-    if (!d_in) CK(stage_input());
-    const bool staged_out = d_out == nullptr;
-    if (staged_out) {
-        CK(ctx->io_out.ensure(std::max<uint64_t>(oend, 16), s));
-        d_out = ctx->io_out.as<uint8_t>();
+    // the staged copy, issued before this point. "Slow": the decode time,
+    // estimated from the stream headers (the largest stream's serial rounds,
+    // about 320 ns per 32 bytes for order-1 and 80 ns for order-0 on B200,
+    // or the whole batch at the batched rates, about 15 and 300 GB/s), keeps
+    // the output rate under 40 GB/s.
+    if (!d_in && in_place > 0) d_in = static_cast<const uint8_t *>(mapped_device_ptr(h_src));
+    if (!d_in && mirror) {
+        double t_lat = 0.0, b0 = 0.0, b1 = 0.0;
+        for (size_t i = 0; i < nblocks; i++) {
+            if (blocks[i].length < kHdr) continue;
+            const uint8_t *h = h_src + blocks[i].offset;
+            uint64_t n = 0;
+            for (int k = 0; k < 8; k++) n |= (uint64_t)h[1 + k] << (8 * k);
+            if (n > out_spans[i].length) continue;
+            const bool o1 = h[0] == 1;
+            t_lat = std::max(t_lat, (double)(n / 32) * (o1 ? 320e-9 : 80e-9));
+            (o1 ? b1 : b0) += (double)n;
+        }
+        const double t_est = std::max(t_lat, b1 / 15e9 + b0 / 300e9);
+        if (t_est > 0.0 && (double)oend / t_est < 40e9)
+            d_in = static_cast<const uint8_t *>(mapped_device_ptr(h_src));
     }
+    if (!d_in) CK(stage_input());
+    // the staging buffer sits at the destination's address modulo 16, so a
+    // stream's staged and final bytes are congruent (16-byte stores)
+    const uint64_t skew = mirror ? (uint64_t)((uintptr_t)h_dst & 15u) : 0u;
+    CK(ctx->io_out.ensure(std::max<uint64_t>(oend + skew, 16), s));
+    uint8_t *d_out = ctx->io_out.as<uint8_t>() + skew;
     std::vector<uint64_t> lens(nblocks);
     std::vector<int32_t> sts(nblocks);
     const int first = decode_batch_impl(ctx, d_in, blocks, nblocks, max_len, d_out, out_spans, lens.data(),
-                                        sts.data(), 1);
+                                        sts.data(), 1, mirror);
     if (first != FQXV_RANS_OK && (first < FQXV_RANS_E_TRUNCATED || first > FQXV_RANS_E_TRUNCATED_RENORM))
         return first;
-    if (!staged_out) {
+    if (mirror) {
         for (size_t i = 0; i < nblocks; i++) {
             if (out_lens) out_lens[i] = lens[i];
             if (status) status[i] = sts[i];
@@ -1003,12 +1041,12 @@ int decode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
     uint64_t produced = 0;
     for (size_t i = 0; i < nblocks; i++) produced += lens[i];
     if (produced == oend && first == FQXV_RANS_OK) {
-        CK(cudaMemcpyAsync(h_dst, ctx->io_out.p, oend, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(h_dst, d_out, oend, cudaMemcpyDeviceToHost, s));
     } else {
         for (size_t i = 0; i < nblocks; i++)
             if (lens[i])
-                CK(cudaMemcpyAsync(h_dst + out_spans[i].offset, ctx->io_out.as<uint8_t>() + out_spans[i].offset,
-                                   lens[i], cudaMemcpyDeviceToHost, s));
+                CK(cudaMemcpyAsync(h_dst + out_spans[i].offset, d_out + out_spans[i].offset, lens[i],
+                                   cudaMemcpyDeviceToHost, s));
     }
     CK(cudaStreamSynchronize(s));
     for (size_t i = 0; i < nblocks; i++) {
@@ -1029,7 +1067,7 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
     if (nblocks == 0) return FQXV_RANS_OK;
     NvtxRange range("fqxv.decode_batch_host");
     std::lock_guard<std::mutex> g(ctx->mu);
-    const auto chunks = pipe_chunks(blocks, nblocks);
+    const auto chunks = pipe_chunks(blocks, nblocks, ctx->tune.host_chunks);
     if (chunks.size() == 1)
         return decode_host_one(ctx, h_src, blocks, nblocks, max_len, h_dst, out_spans, out_lens, status);
     const size_t k = chunks.size();

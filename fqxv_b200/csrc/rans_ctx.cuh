@@ -73,13 +73,15 @@ struct HostBuf {
     }
 };
 
-// Decode launch groups: order-0; order-1 small alphabets; order-1 byte
-// columns in three table-size ranges; the largest order-1 byte-column
-// streams (four-warp decoder) and the largest small-alphabet ones, each of
-// these two on SMs of their own; order-1 global tables.
-constexpr int kGroups = 8;
-constexpr int kGroupFourTop = 5;
-constexpr int kGroupSmallTop = 6;
+// Decode launch groups: order-0; order-1 small alphabets; order-1 wide
+// alphabets in three table-size ranges; the order-1 streams that bound the
+// batch by their serial time, wide alphabets (four-warp decoder) and small
+// ones, each group on SMs of its own; order-1 global tables.
+constexpr int kGroupDense0 = 2;   // first of the three dense table-size groups
+constexpr int kDenseGroups = 3;
+constexpr int kGroupFourTop = kGroupDense0 + kDenseGroups;
+constexpr int kGroupSmallTop = kGroupFourTop + 1;
+constexpr int kGroups = kGroupSmallTop + 2;
 
 enum Stage {
     kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
@@ -113,7 +115,8 @@ struct Tuning {
     // CTAs per SM of each decode class, at most (the occupancy API bounds it too)
     int64_t cta_cap_o0 = 32, cta_cap_o1_small = 32, cta_cap_o1_wide = 32, cta_cap_o1_four = 8,
             cta_cap_o1_global = 32;
-    // table-image sizes cutting dense order-1 streams into launch groups
+    // table-image sizes cutting the other dense wide-alphabet streams into
+    // launch groups (a launch's shared memory is its largest member's)
     int64_t dense_edge_small = 40 << 10, dense_edge_large = 80 << 10;
     // encode kernel grid, CTAs per SM
     int64_t enc_run_ctas_per_sm = 16;
@@ -121,6 +124,15 @@ struct Tuning {
     // (u16) for the encode kernel to read back; 0, the encode kernel derives
     // it from the byte and its predecessor (no per-position array).
     int64_t enc_o1_keys = 1;
+    // Host-buffer calls: chunks a batch of 32 MiB or more is cut into (one
+    // sub-context and host thread each); whether a decode reads its pinned
+    // input in place (-1: when the batch is slow and has hundreds of
+    // streams, 0: never, 1: whenever it is pinned); whether the decoding
+    // CTAs copy each finished stream to a large pinned destination (1) or
+    // the output is copied once the batch is done (0).
+    int64_t host_chunks = 4;
+    int64_t host_in_place = -1;
+    int64_t host_out_mirror = 1;
     std::string source;  // the table file applied (empty: defaults)
 };
 int tuning_set(Tuning &t, const char *key, int64_t value);

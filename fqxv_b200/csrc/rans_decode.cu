@@ -258,7 +258,8 @@ __global__ void __launch_bounds__(kParseThreads)
                     const int stride = nd + 1;
                     const uint32_t cs = dense_col_stride(nd);
                     const bool packed = dense_packed(nd);
-                    uint16_t *M = reinterpret_cast<uint16_t *>(T);
+                    uint8_t *M8 = T;
+                    uint32_t *MB = reinterpret_cast<uint32_t *>(T + kDenseMB);
                     uint32_t *FC = reinterpret_cast<uint32_t *>(T + kDenseM);
                     uint8_t *DS = T + kDenseM + dense_fc_bytes(nd);
                     // byte columns: the image itself, or (packed form) scratch
@@ -271,7 +272,8 @@ __global__ void __launch_bounds__(kParseThreads)
                         reinterpret_cast<uint32_t *>(COL)[i] = deadw;
                     for (int i = tid; i < stride * stride; i += blockDim.x) FC[i] = 0;
                     for (int i = tid; i < (int)kTotFreq; i += blockDim.x)
-                        M[i] = (uint16_t)(packed ? s_col[i] : s_col[i] * (cs >> 4));
+                        M8[i] = (uint8_t)(s_col[i] - s_col[i & ~255]);
+                    if (tid < (int)(kTotFreq / 256)) MB[tid] = packed ? s_col[tid * 256] : s_col[tid * 256] * cs;
                     if (tid < 256 && dmap[tid] != 0xff) DS[dmap[tid]] = (uint8_t)tid;
                     __syncthreads();
                     // One warp per present context: its FC row, and its row
@@ -586,10 +588,28 @@ __device__ __forceinline__ bool o0_general_round(uint32_t &x, const uint32_t *__
     return true;
 }
 
+// Copy of a decoded stream's output to the mirror (the device alias of a
+// pinned host destination), made by the CTA that decoded it as soon as it is
+// done: while other streams still decode, the host link takes the stream in
+// 16-byte stores instead of the kernels' one-byte-per-lane output stores.
+// `src` and `dst` are congruent modulo 16 (the host code places the device
+// staging buffer so); the output was written by this CTA before the barrier
+// that precedes the call, so plain loads see it.
+__device__ __forceinline__ void mirror_out(const uint8_t *src, uint8_t *dst, uint64_t n, int t, int nt) {
+    const uint64_t head = min(n, (uint64_t)((16u - ((uint32_t)(uintptr_t)dst & 15u)) & 15u));
+    for (uint64_t i = t; i < head; i += nt) dst[i] = src[i];
+    const uint64_t body = (n - head) / 16;
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(src + head);
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst + head);
+    for (uint64_t i = t; i < body; i += nt) d4[i] = s4[i];
+    for (uint64_t i = head + 16 * body + t; i < n; i += nt) dst[i] = src[i];
+}
+
 __global__ void __launch_bounds__(32)
     dec_o0_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                   const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
-                  uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t first_polls) {
+                  uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t first_polls,
+                  uint8_t *__restrict__ mirror) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
     const int lane = threadIdx.x;
@@ -673,6 +693,7 @@ __global__ void __launch_bounds__(32)
         }
         if (lane == 0) S.status = status;
         __syncwarp();
+        if (mirror && status == FQXV_RANS_OK) mirror_out(out, mirror + S.dst_off, S.n, lane, 32);
     }
 }
 
@@ -710,15 +731,18 @@ __device__ __forceinline__ void named_bar(int id) {
 // load); packed columns give the column itself, 16 four-bit entries in a
 // u64 (a chain step is then a shift of a register).
 struct ByteCols {
-    const uint16_t *M;
+    const uint8_t *M8;
+    const uint32_t *MB;
+    uint32_t cs;  // column stride, bytes
     using T = uint32_t;
-    __device__ __forceinline__ T operator()(uint32_t slot) const { return (uint32_t)M[slot] << 4; }
+    __device__ __forceinline__ T operator()(uint32_t slot) const { return MB[slot >> 8] + (uint32_t)M8[slot] * cs; }
 };
 struct PackedCols {
-    const uint16_t *M;
+    const uint8_t *M8;
+    const uint32_t *MB;
     const uint64_t *PK;
     using T = uint64_t;
-    __device__ __forceinline__ T operator()(uint32_t slot) const { return PK[M[slot]]; }
+    __device__ __forceinline__ T operator()(uint32_t slot) const { return PK[MB[slot >> 8] + (uint32_t)M8[slot]]; }
 };
 
 // The rounds of one order-1 dense stream (scalar.rs:202-215), shared by the
@@ -843,14 +867,16 @@ static_assert(kPadRow <= kOutRows, "row array too small");
 
 // The parts of a dense table image in shared memory.
 struct DenseImage {
-    const uint16_t *M;     // slot -> column offset in 16-byte units
+    const uint8_t *M8;     // slot -> column, less its 256-slot block's first column
+    const uint32_t *MB;    // per 256-slot block: its first column (byte offset for byte columns)
     const uint8_t *COL;    // columns
     const uint32_t *FC;    // (freq << 12) | cum per (context, symbol)
     const uint8_t *DS;     // dense index -> byte
     uint32_t stride;       // FC row stride (nd + 1)
     uint32_t dead;
     __device__ DenseImage(const uint8_t *sm, int nd)
-        : M(reinterpret_cast<const uint16_t *>(sm)),
+        : M8(sm),
+          MB(reinterpret_cast<const uint32_t *>(sm + kDenseMB)),
           COL(sm + dense_col_off(nd)),
           FC(reinterpret_cast<const uint32_t *>(sm + kDenseM)),
           DS(sm + kDenseM + dense_fc_bytes(nd)),
@@ -941,7 +967,7 @@ __device__ __forceinline__ int o1d_stream(DecStream &S, const uint8_t *__restric
         buf ^= 1u;
     };
 
-    return o1_rounds(S, R, out, lt, ByteCols{I.M}, I.FC, I.DS, I.stride, dead, warp == 0, x, resolve);
+    return o1_rounds(S, R, out, lt, ByteCols{I.M8, I.MB, dense_col_stride(nd)}, I.FC, I.DS, I.stride, dead, warp == 0, x, resolve);
 }
 
 // Four-warp decode of a stream with bit-plane columns (kSmallMaxNd < |D| <=
@@ -1032,14 +1058,14 @@ __device__ __forceinline__ int o1p_stream(DecStream &S, const uint8_t *__restric
         buf ^= 1u;
     };
 
-    return o1_rounds(S, R, out, lt, ByteCols{I.M}, I.FC, I.DS, I.stride, dead, warp == 0, S.states[lane], resolve);
+    return o1_rounds(S, R, out, lt, ByteCols{I.M8, I.MB, dense_col_stride(nd)}, I.FC, I.DS, I.stride, dead, warp == 0, S.states[lane], resolve);
 }
 
 __global__ void __launch_bounds__(kO1Threads, 1)
     dec_o1d_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
                    uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off,
-                   uint32_t first_polls) {
+                   uint32_t first_polls, uint8_t *__restrict__ mirror) {
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ __align__(16) uint4 s_rows[2][kOutRows + 1];
@@ -1079,6 +1105,7 @@ __global__ void __launch_bounds__(kO1Threads, 1)
                                                             : o1d_stream<2>(S, sm, R, s_rows, out, lt);
         if (tid == 0) S.status = status;
         __syncthreads();
+        if (mirror && status == FQXV_RANS_OK) mirror_out(out, mirror + S.dst_off, S.n, tid, kO1Threads);
     }
 }
 
@@ -1174,7 +1201,7 @@ __device__ __forceinline__ int o1s_stream(DecStream &S, const uint8_t *__restric
         ctx = pos == 0 ? in : ((pos <= 4 ? row_x : row_y) >> shc) & 0xffu;
         din = r3y & 0xffu;
     };
-    return o1_rounds(S, R, out, lt, PackedCols{I.M, PK}, I.FC, I.DS, I.stride, dead, true, S.states[lane],
+    return o1_rounds(S, R, out, lt, PackedCols{I.M8, I.MB, PK}, I.FC, I.DS, I.stride, dead, true, S.states[lane],
                      resolve);
 }
 
@@ -1275,10 +1302,10 @@ __device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restric
         buf ^= 1u;
     };
     if constexpr (PACKED)
-        return o1_rounds(S, R, out, lt, PackedCols{I.M, reinterpret_cast<const uint64_t *>(I.COL)}, I.FC, I.DS,
+        return o1_rounds(S, R, out, lt, PackedCols{I.M8, I.MB, reinterpret_cast<const uint64_t *>(I.COL)}, I.FC, I.DS,
                          I.stride, dead, true, S.states[lane], resolve);
     else
-        return o1_rounds(S, R, out, lt, ByteCols{I.M}, I.FC, I.DS, I.stride, dead, true, S.states[lane], resolve);
+        return o1_rounds(S, R, out, lt, ByteCols{I.M8, I.MB, dense_col_stride(nd)}, I.FC, I.DS, I.stride, dead, true, S.states[lane], resolve);
 }
 
 // The two one-warp order-1 decoders: the small class (packed columns:
@@ -1290,7 +1317,7 @@ __global__ void __launch_bounds__(32)
     dec_o1w_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
                    uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off,
-                   uint32_t first_polls) {
+                   uint32_t first_polls, uint8_t *__restrict__ mirror) {
     constexpr int kRows = 3 * (kWide ? kDenseMax : kSmallMaxNd) + 2;
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -1331,6 +1358,7 @@ __global__ void __launch_bounds__(32)
         }
         if (lane == 0) S.status = status;
         __syncwarp();
+        if (mirror && status == FQXV_RANS_OK) mirror_out(out, mirror + S.dst_off, S.n, lane, 32);
     }
 }
 static_assert((kDenseMax + kWideLanes - 1) / kWideLanes <= 5, "o1w_stream instantiations cover TPL <= 5");
@@ -1345,7 +1373,7 @@ static_assert(3 * kShflMaxNd + 1 <= 31, "shuffle-resolved chains fit in a warp")
 __global__ void __launch_bounds__(32)
     dec_o1g_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
-                   uint8_t *__restrict__ dst, int *__restrict__ queue) {
+                   uint8_t *__restrict__ dst, int *__restrict__ queue, uint8_t *__restrict__ mirror) {
     extern __shared__ __align__(128) uint8_t sm[];
     const int lane = threadIdx.x;
     const uint32_t lt = lanemask_lt();
@@ -1414,6 +1442,7 @@ __global__ void __launch_bounds__(32)
         }
         if (lane == 0) S.status = status;
         __syncwarp();
+        if (mirror && status == FQXV_RANS_OK) mirror_out(out, mirror + S.dst_off, S.n, lane, 32);
     }
 }
 
@@ -1528,27 +1557,29 @@ void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint
 
 void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
-                    uint32_t first_polls, cudaStream_t s) {
+                    uint32_t first_polls, uint8_t *mirror, cudaStream_t s) {
     if (nlist <= 0 || grid <= 0) return;
     ensure_dec_attrs();
     switch (cls) {
         case kClsO0:
-            dec_o0_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue, first_polls);
+            dec_o0_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue, first_polls,
+                                                       mirror);
             break;
         case kClsO1Dense:
             dec_o1d_kernel<<<grid, kO1Threads, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                                smem_bytes - kO1Warps * kRingBytes, first_polls);
+                                                                smem_bytes - kO1Warps * kRingBytes, first_polls,
+                                                                mirror);
             break;
         case kClsO1Global:
-            dec_o1g_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue);
+            dec_o1g_kernel<<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue, mirror);
             break;
         case kClsO1Small:
             dec_o1w_kernel<false><<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                                smem_bytes - kRingBytes, first_polls);
+                                                                smem_bytes - kRingBytes, first_polls, mirror);
             break;
         case kClsO1Wide:
             dec_o1w_kernel<true><<<grid, 32, smem_bytes, s>>>(src, streams, list, nlist, tbl, dst, queue,
-                                                               smem_bytes - kRingBytes, first_polls);
+                                                               smem_bytes - kRingBytes, first_polls, mirror);
             break;
         default:
             break;

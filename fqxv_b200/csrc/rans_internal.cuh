@@ -114,17 +114,20 @@ constexpr int kShflMaxNd = 10;
 //     boundary: a cum value of a present symbol); between two boundaries
 //     every context decodes every slot to the same symbol, so one column per
 //     boundary holds, for each context, the dense symbol of that slot range.
-//     [0, 8192)                 M: u16 per slot, the column of the slot in
-//                               16-byte units (column j * S / 16)
-//     [8192, + fc_bytes)        u32 (freq << 12) | cum, row = context, col = symbol
+//     [0, 4096)                 M8: u8 per slot, the slot's column less the
+//                               first column of its 256-slot block
+//     [4096, 4160)              MB: u32 per 256-slot block, that first
+//                               column (times S for byte columns: a byte
+//                               offset)
+//     [4160, + fc_bytes)        u32 (freq << 12) | cum, row = context, col = symbol
 //     [.., + 256)               dense index -> byte value
 //     [col_off, + ncol * S)     columns, S = dense_col_stride(nd) bytes each:
 //                               byte d of column j = the dense symbol that
 //                               context d decodes in column j's slots (DEAD
 //                               for rows of absent contexts and for DEAD)
-//     Full-range quality tables (|D| ~ 31) have ~480 columns: ~28 KB against
+//     Full-range quality tables (|D| ~ 31) have ~480 columns: ~23 KB against
 //     ~130 KB for a slot -> symbol table per context.
-//     Packed form, |D| <= kSmallMaxNd: M holds the column index j, and the
+//     Packed form, |D| <= kSmallMaxNd: MB holds plain column indices, and the
 //     columns are u64 at col_off, entry d in bits [4d, 4d + 4), so a chain
 //     step is a shift of a register instead of a shared-memory load.
 //   order-1 global (more symbols, or more columns than the image holds):
@@ -132,7 +135,8 @@ constexpr int kShflMaxNd = 10;
 //     context t: 4096 x u16 (sym << 8) | dense(sym), then 256 x u32
 //     (freq << 12) | cum.
 constexpr int kDenseMax = 47;
-constexpr uint32_t kDenseM = 8192;
+constexpr uint32_t kDenseMB = 4096;          // M8: u8 per slot
+constexpr uint32_t kDenseM = kDenseMB + 64;  // MB: u32 per 256-slot block
 constexpr uint32_t kDenseImageMax = 160 * 1024;
 __host__ __device__ inline uint32_t dense_col_stride(int nd) { return (uint32_t)((nd + 1 + 15) / 16 * 16); }
 __host__ __device__ inline uint32_t dense_fc_bytes(int nd) {
@@ -203,9 +207,12 @@ void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint
                       int grid, cudaStream_t s);
 // Runs the decode of the streams listed in `list` (all of class `cls`);
 // smem_bytes is the dynamic shared memory of the class (largest member).
+// `mirror` (nullable): each stream decoded without error is also copied to
+// mirror + dst_off (the device alias of a pinned host destination) by the
+// CTA that decoded it.
 void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
-                    uint32_t first_polls, cudaStream_t s);
+                    uint32_t first_polls, uint8_t *mirror, cudaStream_t s);
 uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes);
 // Dynamic shared memory with which one CTA of a decode class fills an SM (no
 // other CTA fits beside it); 0 when the class cannot.

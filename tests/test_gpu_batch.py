@@ -199,6 +199,39 @@ def test_host_decode_pinned_and_pageable_agree(codec, orc):
             assert page_dst[o:o + int(l2[i])].tobytes() == wb
 
 
+def test_pinned_destination_mirror_unaligned(codec, orc):
+    """A large pinned destination is filled by the decoding CTAs' copies of
+    their streams (16-byte stores between ragged ends): a destination that
+    starts at an odd address, streams back to back at odd offsets, lengths
+    from 1 byte up, both orders and a truncated stream in the middle."""
+    import torch
+
+    rng = np.random.default_rng(19)
+    blocks = [W.GENERATORS[list(W.GENERATORS)[i % 4]](n, 70 + i)
+              for i, n in enumerate([1, 2, 15, 16, 17, 31, 33, 1000, 70_001, 300_000, 1 << 20, 2_500_001])]
+    blocks += [W.GENERATORS["full"](int(rng.integers(1, 400_000)), 90 + i) for i in range(20)]
+    streams = [orc.encode(b.tobytes(), i % 2) for i, b in enumerate(blocks)]
+    streams[9] = streams[9][:len(streams[9]) // 3]
+    lens = np.array([len(x) for x in streams], np.uint64)
+    offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint64)
+    nout = np.array([len(b) for b in blocks], np.uint64)
+    doffs = np.concatenate([[0], np.cumsum(nout)[:-1]]).astype(np.uint64)
+    total = int(nout.sum())
+    assert total >= (4 << 20)
+    h_in = torch.from_numpy(np.frombuffer(b"".join(streams), np.uint8).copy()).pin_memory().numpy()
+    pinned = torch.zeros(total + 64, dtype=torch.uint8).pin_memory().numpy()
+    h_dst = pinned[5:5 + total]
+    l, st = codec.decode_batch_host(h_in, np.stack([offs, lens], 1), np.stack([doffs, nout], 1), h_dst,
+                                    raise_on_error=False)
+    for i, b in enumerate(blocks):
+        ws, wb = orc.decode_status(streams[i])
+        assert st[i] == ws, i
+        if ws == 0:
+            o = int(doffs[i])
+            assert h_dst[o:o + int(l[i])].tobytes() == wb == b.tobytes(), i
+    assert not pinned[:5].any() and not pinned[5 + total:].any()
+
+
 def test_small_alphabet_order1_statuses_match_oracle(codec, orc):
     """Order-1 streams of small alphabets (the one-warp decoder): good,
     truncated and corrupted streams give the oracle's bytes and statuses."""
@@ -281,7 +314,8 @@ def test_launch_shapes_change_no_byte(codec):
     settings = [
         {"o1_four_max_streams": 0, "cta_cap_o1_wide": 1, "enc_run_ctas_per_sm": 4},
         {"o1_four_max_streams": 1 << 30, "cta_cap_o1_four": 1, "dense_edge_small": 0, "dense_edge_large": 0},
-        {"cta_cap_o0": 1, "cta_cap_o1_small": 2, "dense_edge_small": 160 << 10, "dense_edge_large": 160 << 10},
+        {"cta_cap_o0": 1, "cta_cap_o1_small": 2, "cta_cap_o1_wide": 3, "dense_edge_small": 160 << 10,
+         "dense_edge_large": 160 << 10},
         {"o1_top_exclusive": 0, "o1_top_max": 0, "enc_o1_keys": 0},
         {"o1_top_exclusive": 1, "o1_top_max": 5, "o1_top_latency_pct": 0},
         {"o1_top_exclusive": 1, "o1_top_max": 1 << 20, "o1_top_latency_pct": 0, "enc_o1_keys": 0},
