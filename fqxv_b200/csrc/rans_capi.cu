@@ -333,6 +333,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
         uint32_t tmax[kGroups] = {}, tmaxp[kGroups] = {};
         uint64_t cbytes[kGroups] = {};
         uint64_t maxn[kGroups] = {};
+        int ndmax[kGroups] = {};
         for (uint32_t i : ord) {
             const int g = group_of(i);
             if (g < 0) continue;
@@ -341,6 +342,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             tmaxp[g] = std::max(tmaxp[g], ps[i].tbl_bytes_planes);
             cbytes[g] += ps[i].src_len + ps[i].n;
             maxn[g] = std::max<uint64_t>(maxn[g], ps[i].n);
+            ndmax[g] = std::max(ndmax[g], ps[i].nd);
         }
         int gcls[kGroups];
         uint32_t smem[kGroups];
@@ -352,7 +354,7 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             else if (g == kGroupFourTop) gcls[g] = kClsO1Dense;
             else gcls[g] = (int64_t)lists[g].size() < four_max ? kClsO1Dense : kClsO1Wide;
             // the four-warp decoder also stages the bit-plane columns
-            smem[g] = dec_smem_bytes(gcls[g], gcls[g] == kClsO1Dense ? tmaxp[g] : tmax[g]);
+            smem[g] = dec_smem_bytes(gcls[g], gcls[g] == kClsO1Dense ? tmaxp[g] : tmax[g], ndmax[g]);
             // the groups of largest streams: one CTA per SM, alone on it
             if ((g == kGroupFourTop || g == kGroupSmallTop) && ctx->tune.o1_top_exclusive)
                 smem[g] = std::max(smem[g], dec_exclusive_smem(gcls[g]));
@@ -408,7 +410,8 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
                     cudaEvent_t t0 = ctx->timer.begin(as);
                     launch_dec_run(cls, d_src, dS, dl + base[g] + j, 1, dT, d_dst, queue + 4 * g, 1,
                                    dec_smem_bytes(cls, cls == kClsO1Dense ? ps[lists[g][j]].tbl_bytes_planes
-                                                                          : ps[lists[g][j]].tbl_bytes),
+                                                                          : ps[lists[g][j]].tbl_bytes,
+                                                  ps[lists[g][j]].nd),
                                    ctx->first_polls, mirror, as);
                     ctx->timer.end(stage, t0, as);
                 }
@@ -798,9 +801,9 @@ int encode_host_one(fqxv_rans_ctx *ctx, const uint8_t *h_src, const fqxv_rans_sp
 }
 
 // Host-buffer batches of at least kPipeMinBytes are cut into up to
-// `host_chunks` chunks of consecutive blocks, each coded by its own
-// sub-context on its own host thread: one chunk's copies overlap the other
-// chunks' kernels, and chunks of equal blocks run side by side on the GPU.
+// `host_enc_chunks` (encode) or `host_dec_chunks` (decode) chunks of
+// consecutive blocks, each coded by its own sub-context on its own host
+// thread: one chunk's copies overlap the other chunks' kernels.
 constexpr uint64_t kPipeMinBytes = 32ull << 20;
 
 // [first, last) block ranges of roughly equal bytes
@@ -863,7 +866,7 @@ int fqxv_rans_encode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
     if (nblocks == 0) return FQXV_RANS_OK;
     NvtxRange range("fqxv.encode_batch_host");
     std::lock_guard<std::mutex> g(ctx->mu);
-    const auto chunks = pipe_chunks(blocks, nblocks, ctx->tune.host_chunks);
+    const auto chunks = pipe_chunks(blocks, nblocks, ctx->tune.host_enc_chunks);
     if (chunks.size() == 1) {
         return encode_host_one(ctx, h_src, blocks, nblocks, order, out_spans, out_orders,
                                [&](int st, uint64_t total, uint8_t *&dst) -> int {
@@ -1067,7 +1070,7 @@ int fqxv_rans_decode_batch_host(fqxv_rans_ctx *ctx, const uint8_t *h_src, const 
     if (nblocks == 0) return FQXV_RANS_OK;
     NvtxRange range("fqxv.decode_batch_host");
     std::lock_guard<std::mutex> g(ctx->mu);
-    const auto chunks = pipe_chunks(blocks, nblocks, ctx->tune.host_chunks);
+    const auto chunks = pipe_chunks(blocks, nblocks, ctx->tune.host_dec_chunks);
     if (chunks.size() == 1)
         return decode_host_one(ctx, h_src, blocks, nblocks, max_len, h_dst, out_spans, out_lens, status);
     const size_t k = chunks.size();

@@ -125,12 +125,16 @@ struct Tuning {
     // it from the byte and its predecessor (no per-position array).
     int64_t enc_o1_keys = 1;
     // Host-buffer calls: chunks a batch of 32 MiB or more is cut into (one
-    // sub-context and host thread each); whether a decode reads its pinned
+    // sub-context and host thread each), for encode (the input copy of one
+    // chunk overlaps the encode of the one before) and decode (a decode is
+    // bound by its longest streams, and chunks decoded side by side slowed
+    // config2's host decode from 74 to 123 ms); whether a decode reads its pinned
     // input in place (-1: when the batch is slow and has hundreds of
     // streams, 0: never, 1: whenever it is pinned); whether the decoding
     // CTAs copy each finished stream to a large pinned destination (1) or
     // the output is copied once the batch is done (0).
-    int64_t host_chunks = 4;
+    int64_t host_enc_chunks = 4;
+    int64_t host_dec_chunks = 1;
     int64_t host_in_place = -1;
     int64_t host_out_mirror = 1;
     std::string source;  // the table file applied (empty: defaults)

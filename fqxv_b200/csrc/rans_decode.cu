@@ -1311,14 +1311,18 @@ __device__ __forceinline__ int o1w_stream(DecStream &S, const uint8_t *__restric
 // The two one-warp order-1 decoders: the small class (packed columns:
 // o1s_stream up to kShflMaxNd symbols, o1w_stream<2, packed> up to
 // kSmallMaxNd) and the wide class (byte columns, o1w_stream<TPL>). Row
-// arrays: 3 nd + 2 rows per buffer.
+// arrays: 3 nd + 2 rows per buffer; the small class keeps them in static
+// shared memory, the wide class right below its word ring in dynamic shared
+// memory, sized for the stream's own |D| (the launch reserves them for the
+// largest |D| among its streams), so a full-range stream's CTA is ~1.5 KB
+// smaller than with rows for |D| = kDenseMax.
 template <bool kWide>
 __global__ void __launch_bounds__(32)
     dec_o1w_kernel(const uint8_t *__restrict__ src, DecStream *__restrict__ streams,
                    const uint32_t *__restrict__ list, int nlist, const uint8_t *__restrict__ tbl,
                    uint8_t *__restrict__ dst, int *__restrict__ queue, uint32_t ring_off,
                    uint32_t first_polls, uint8_t *__restrict__ mirror) {
-    constexpr int kRows = 3 * (kWide ? kDenseMax : kSmallMaxNd) + 2;
+    constexpr int kRows = kWide ? 1 : 3 * kSmallMaxNd + 2;
     extern __shared__ __align__(128) uint8_t sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ __align__(16) uint4 s_rows[2][kRows];
@@ -1347,10 +1351,12 @@ __global__ void __launch_bounds__(32)
         int status;
         if constexpr (kWide) {
             const int tpl = (S.nd + kWideLanes - 1) / kWideLanes;
-            status = tpl <= 2   ? o1w_stream<2, false>(S, sm, R, s_rows[0], s_rows[1], out, lt)
-                     : tpl == 3 ? o1w_stream<3, false>(S, sm, R, s_rows[0], s_rows[1], out, lt)
-                     : tpl == 4 ? o1w_stream<4, false>(S, sm, R, s_rows[0], s_rows[1], out, lt)
-                                : o1w_stream<5, false>(S, sm, R, s_rows[0], s_rows[1], out, lt);
+            uint4 *r0 = reinterpret_cast<uint4 *>(sm + ring_off - wide_rows_bytes(S.nd));
+            uint4 *r1 = r0 + (3 * S.nd + 2);
+            status = tpl <= 2   ? o1w_stream<2, false>(S, sm, R, r0, r1, out, lt)
+                     : tpl == 3 ? o1w_stream<3, false>(S, sm, R, r0, r1, out, lt)
+                     : tpl == 4 ? o1w_stream<4, false>(S, sm, R, r0, r1, out, lt)
+                                : o1w_stream<5, false>(S, sm, R, r0, r1, out, lt);
         } else {
             status = S.nd <= 7            ? o1s_stream<true>(S, sm, R, out, lt)
                      : S.nd <= kShflMaxNd ? o1s_stream<false>(S, sm, R, out, lt)
@@ -1450,13 +1456,13 @@ __global__ void __launch_bounds__(32)
 // launchers
 // ---------------------------------------------------------------------------
 
-uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes) {
+uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes, int nd) {
     switch (cls) {
         case kClsO0: return 16384 + kRingBytes;
         case kClsO1Dense: return (uint32_t)align_up(tbl_bytes, 128) + kO1Warps * kRingBytes;
         case kClsO1Global: return kRingBytes;
-        case kClsO1Small:
-        case kClsO1Wide: return (uint32_t)align_up(tbl_bytes, 128) + kRingBytes;
+        case kClsO1Small: return (uint32_t)align_up(tbl_bytes, 128) + kRingBytes;
+        case kClsO1Wide: return (uint32_t)align_up(tbl_bytes, 128) + wide_rows_bytes(nd) + kRingBytes;
         default: return 0;
     }
 }

@@ -213,7 +213,11 @@ void launch_dec_parse(const uint8_t *src, DecStream *streams, int nstreams, uint
 void launch_dec_run(int cls, const uint8_t *src, DecStream *streams, const uint32_t *list, int nlist,
                     const uint8_t *tbl, uint8_t *dst, int *queue, int grid, uint32_t smem_bytes,
                     uint32_t first_polls, uint8_t *mirror, cudaStream_t s);
-uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes);
+// `nd`: the largest |D| among the launch's streams (the one-warp wide
+// decoder keeps its rows, 3 |D| + 2 per buffer, in dynamic shared memory).
+uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes, int nd = kDenseMax);
+// Bytes of the one-warp wide decoder's two row buffers for |D| = nd.
+__host__ __device__ inline uint32_t wide_rows_bytes(int nd) { return (uint32_t)((2 * (3 * nd + 2) * 16 + 127) / 128 * 128); }
 // Dynamic shared memory with which one CTA of a decode class fills an SM (no
 // other CTA fits beside it); 0 when the class cannot.
 uint32_t dec_exclusive_smem(int cls);

@@ -46,7 +46,8 @@ const ParamDef kParams[] = {
     {"dense_edge_large", &Tuning::dense_edge_large, 0, kDenseImageMax},
     {"enc_run_ctas_per_sm", &Tuning::enc_run_ctas_per_sm, 1, 64},
     {"enc_o1_keys", &Tuning::enc_o1_keys, 0, 1},
-    {"host_chunks", &Tuning::host_chunks, 1, 16},
+    {"host_enc_chunks", &Tuning::host_enc_chunks, 1, 16},
+    {"host_dec_chunks", &Tuning::host_dec_chunks, 1, 16},
     {"host_in_place", &Tuning::host_in_place, -1, 1},
     {"host_out_mirror", &Tuning::host_out_mirror, 0, 1},
 };

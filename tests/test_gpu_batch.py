@@ -290,7 +290,12 @@ def test_host_batches_in_chunks_match_single_pass(codec, orc):
     bad[37, 1] = bad[37, 1] // 2
     h_in = torch.from_numpy(enc).pin_memory().numpy()
     h_dec = torch.zeros(len(data), dtype=torch.uint8).pin_memory().numpy()
-    lens, st = codec.decode_batch_host(h_in, bad, spans, h_dec, raise_on_error=False)
+    old = codec.get_param("host_dec_chunks")
+    codec.set_param("host_dec_chunks", 4)
+    try:
+        lens, st = codec.decode_batch_host(h_in, bad, spans, h_dec, raise_on_error=False)
+    finally:
+        codec.set_param("host_dec_chunks", old)
     stream37 = enc[int(bad[37, 0]):int(bad[37, 0] + bad[37, 1])].tobytes()
     assert st[37] == orc.decode_status(stream37)[0] != 0
     for i in range(40):

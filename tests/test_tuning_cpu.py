@@ -22,7 +22,8 @@ KNOWN = {
     "dense_edge_large": (0, 160 * 1024),
     "enc_run_ctas_per_sm": (1, 64),
     "enc_o1_keys": (0, 1),
-    "host_chunks": (1, 16),
+    "host_enc_chunks": (1, 16),
+    "host_dec_chunks": (1, 16),
     "host_in_place": (-1, 1),
     "host_out_mirror": (0, 1),
 }
