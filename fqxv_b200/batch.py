@@ -302,9 +302,9 @@ class Codec:
         rans.raise_for(self._lib.fqxv_rans_ctx_set_profiling(self._h, 1 if on else 0))
 
     def stage_stats(self, reset: bool = False) -> dict:
-        arr = (StageStat * 16)()
+        arr = (StageStat * 32)()
         n = ctypes.c_int(0)
-        rans.raise_for(self._lib.fqxv_rans_ctx_stage_stats(self._h, ctypes.cast(arr, ctypes.c_void_p), 16,
+        rans.raise_for(self._lib.fqxv_rans_ctx_stage_stats(self._h, ctypes.cast(arr, ctypes.c_void_p), 32,
                                                            ctypes.byref(n), 1 if reset else 0))
         return {arr[i].name.decode(): {"launches": int(arr[i].launches), "ms": float(arr[i].ms),
                                        "bytes": int(arr[i].bytes), "wall_ms": float(arr[i].wall_ms),

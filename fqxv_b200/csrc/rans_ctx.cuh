@@ -85,12 +85,12 @@ constexpr int kGroups = kGroupSmallTop + 2;
 
 enum Stage {
     kStEncModel, kStEncRun, kStEncScan, kStEncPack, kStDecParse, kStDecO0, kStDecO1Dense, kStDecO1Global,
-    kStDecO1Small, kStDecO1Wide, kStCrcPlan, kStCrc, kStFrameCopy, kStFrameWalk, kStages
+    kStDecO1Small, kStDecO1Wide, kStCrcPlan, kStCrc, kStFrameCopy, kStFrameWalk, kStXEncode, kStXDecode, kStages
 };
 const char *const kStageNames[kStages] = {"enc_model", "enc_run", "enc_select_scan", "enc_pack",
                                           "dec_parse", "dec_o0", "dec_o1_dense", "dec_o1_global",
                                           "dec_o1_small", "dec_o1_wide", "crc_plan", "crc32c",
-                                          "frame_copy_crc", "frame_walk"};
+                                          "frame_copy_crc", "frame_walk", "x_encode", "x_decode"};
 
 // Launch-shape parameters of a context (rans_tuning.cu): defaults are the
 // library's run-time rules; a tuning table measured on the device replaces

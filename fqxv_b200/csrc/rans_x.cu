@@ -292,13 +292,19 @@ __global__ void __launch_bounds__(256) x_unstripe_kernel(const uint8_t *__restri
 
 // ---- 4-state cores ---------------------------------------------------------
 
-// One thread per core: the reverse encode of scalar.rs:29-111 with 4 states
-// (state i % 4 codes position i), tables from the model kernel, words
-// written back to front below word_off + n (decode order when done).
+// One warp per core, lanes 0-3 holding states 0-3: the reverse encode of
+// scalar.rs:29-111 with 4 states (state i % 4 codes position i), tables from
+// the model kernel. A round is positions 4r .. 4r + 3, coded from the top
+// round down; the CPU definition emits position 4r + 3's word first, so
+// stored below the write pointer the round's words land in ascending lane
+// order, handed out by a vote. The next round's table entries are loaded
+// before this round's state updates. Words end below word_off + n, in
+// decode order.
 __global__ void __launch_bounds__(128) x_n4_run_kernel(const uint8_t *__restrict__ src, EncBlock *__restrict__ blocks,
                                                         int nblocks, const uint8_t *__restrict__ tbl,
                                                         uint16_t *__restrict__ words) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int b = blockIdx.x * 4 + (int)(threadIdx.x >> 5);
     if (b >= nblocks) return;
     EncBlock &B = blocks[b];
     const uint64_t n = B.n;
@@ -309,35 +315,56 @@ __global__ void __launch_bounds__(128) x_n4_run_kernel(const uint8_t *__restrict
     const uint2 *T1 = reinterpret_cast<const uint2 *>(T + kTblO1);
     const uint8_t *um = T + kTblUmap;
     const uint32_t nu = (uint32_t)B.nu;
-    uint32_t x[4] = {kRansL, kRansL, kRansL, kRansL};
-    uint16_t *end = words + B.word_off[o] + n;
+    const uint32_t lt = (1u << lane) - 1u;
+    auto entry = [&](uint64_t i) -> uint2 {
+        const uint32_t sy = p[i];
+        if (o == 0) return T0[sy];
+        const uint32_t c = i ? p[i - 1] : 0u;
+        return T1[(size_t)um[c] * nu + um[sy]];
+    };
+    uint32_t x = kRansL;
+    uint16_t *const end = words + B.word_off[o] + n;
     uint16_t *w = end;
-    for (uint64_t i = n; i-- > 0;) {
-        const uint32_t s = p[i];
-        uint2 e;
-        if (o == 0) {
-            e = T0[s];
-        } else {
-            const uint32_t c = i ? p[i - 1] : 0u;
-            e = T1[(size_t)um[c] * nu + um[s]];
-        }
+    // one position of lane's state: emits the pre-step low 16 bits when the
+    // state would pass x_max = f << 20 (never for f = 4096)
+    auto step = [&](uint2 e, bool active) {
         const uint32_t f = e.y >> kScaleBits, cum = e.y & (kTotFreq - 1);
-        uint32_t v = x[i & 3];
-        if ((uint64_t)v >= ((uint64_t)f << 20)) {  // x_max = f << 20 (2^32 for f = 4096: never reached)
-            *--w = (uint16_t)v;
+        uint32_t v = x;
+        const bool need = active && (uint64_t)v >= ((uint64_t)f << 20);
+        const uint32_t mask = __ballot_sync(0xffffffffu, need);
+        w -= __popc(mask);
+        if (need) {
+            w[__popc(mask & lt)] = (uint16_t)v;
             v >>= 16;
         }
-        uint32_t q = __umulhi(v, e.x);
-        uint32_t r = v - q * f;
-        if (r >= f) {
-            q++;
-            r -= f;
+        if (active) {
+            uint32_t q = __umulhi(v, e.x);
+            uint32_t r = v - q * f;
+            if (r >= f) {
+                q++;
+                r -= f;
+            }
+            x = (q << kScaleBits) + r + cum;
         }
-        x[i & 3] = (q << kScaleBits) + r + cum;
+    };
+    const uint64_t full = n / 4;
+    const uint32_t rem = (uint32_t)(n % 4);
+    if (rem) {
+        const bool active = lane < (int)rem;
+        step(active ? entry(4 * full + lane) : make_uint2(0u, 0u), active);
     }
-    for (int k = 0; k < 4; k++) B.states[o][k] = x[k];
-    B.nwords[o] = (uint64_t)(end - w);
-    B.chosen = o;
+    const bool mine = lane < 4;
+    uint2 e = (full && mine) ? entry(4 * (full - 1) + lane) : make_uint2(0u, 0u);
+    for (uint64_t r = full; r-- > 0;) {
+        const uint2 en = (r && mine) ? entry(4 * (r - 1) + lane) : make_uint2(0u, 0u);
+        step(e, mine);
+        e = en;
+    }
+    if (mine) B.states[o][lane] = x;
+    if (lane == 0) {
+        B.nwords[o] = (uint64_t)(end - w);
+        B.chosen = o;
+    }
 }
 
 // Writes one 4-state core per block: [2 | order][u64 n][tables][4 states][words].
@@ -420,8 +447,9 @@ __global__ void __launch_bounds__(256) x_n4_pack_kernel(const EncBlock *__restri
 
 // Decode side of a 4-state core. One CTA per core: its tables checked in the
 // reference's order (model.rs:160-174, scalar.rs:180-198) and expanded into
-// slot -> symbol rows in global scratch, then thread 0 runs the serial chain
-// (scalar.rs:200-238 with 4 states). Statuses as the CPU definition.
+// slot -> symbol rows (in shared memory when the launch reserved room for
+// the core's tables, else in global scratch), then the chain of
+// scalar.rs:200-238 with 4 states. Statuses as the CPU definition.
 struct XN4Dec {
     uint64_t src_off, len;    // the core stream
     uint64_t dst_off, cap;    // its output
@@ -431,10 +459,12 @@ struct XN4Dec {
     int32_t pad;
 };
 constexpr uint64_t kN4Row = 4096 + 1024;
+constexpr uint64_t kN4SmemRows = 32;
 
 __global__ void __launch_bounds__(256) x_n4_decode_kernel(const uint8_t *__restrict__ src, XN4Dec *__restrict__ cores,
                                                            int ncores, uint8_t *__restrict__ scratch,
-                                                           uint8_t *__restrict__ dst) {
+                                                           uint8_t *__restrict__ dst, int ksm) {
+    extern __shared__ __align__(16) uint8_t xsm[];  // ksm rows: cores of at most ksm tables keep them here
     __shared__ uint16_t ctxidx[256];
     __shared__ int s_k;
     __shared__ uint32_t wsum[8];
@@ -472,7 +502,7 @@ __global__ void __launch_bounds__(256) x_n4_decode_kernel(const uint8_t *__restr
         }
         __syncthreads();
         const int K = s_k;
-        uint8_t *rows = scratch + C.scratch_off;
+        uint8_t *rows = K <= ksm ? xsm : scratch + C.scratch_off;
         // one table at a time by the whole CTA: the first failing table
         // decides the status, as the sequential reads do
         for (int t = 0; t < K && status == FQXV_RANS_OK; t++) {
@@ -504,14 +534,60 @@ __global__ void __launch_bounds__(256) x_n4_decode_kernel(const uint8_t *__restr
         if (status == FQXV_RANS_OK && L < pos + 16) status = FQXV_RANS_E_TRUNCATED;
         if (status == FQXV_RANS_OK && n > C.cap) status = FQXV_RANS_E_ALLOC;
         __syncthreads();
+        // Order-0 cores: lanes 0-3 of warp 0 hold the four states and decode
+        // a round of four positions at once; the round's renorm words are
+        // handed out in lane order by a vote (one word at most per state:
+        // once every state is at least 2^16, v = f (x >> 12) + slot - cum is
+        // at least 16, so one 16-bit word lifts it past 2^16 again). Rounds
+        // run this way while a whole round and its four words fit; thread 0
+        // finishes the rest, and order-1 cores (a chain of contexts), one
+        // position at a time with every check of the CPU definition.
+        uint32_t xl = 0;
+        uint64_t i0 = 0;
+        if (warp == 0 && status == FQXV_RANS_OK) {
+            if (lane < 4) xl = ld_u32_le(p + pos + 4 * lane);
+            const bool fast = order == 0 && __all_sync(0xffffffffu, lane >= 4 || xl >= kRansL);
+            if (fast) {
+                const uint8_t *row = rows;
+                const uint32_t *fcr = reinterpret_cast<const uint32_t *>(rows + 4096);
+                uint8_t *out = dst + C.dst_off;
+                const uint32_t lt = (1u << lane) - 1u;
+                uint64_t wp = pos + 16;
+                while (i0 + 4 <= n && wp + 8 <= L) {
+                    uint32_t sy = 0, v = 0;
+                    bool need = false;
+                    if (lane < 4) {
+                        const uint32_t slot = xl & (kTotFreq - 1);
+                        sy = row[slot];
+                        const uint32_t fc = fcr[sy];
+                        v = (fc >> kScaleBits) * (xl >> kScaleBits) + slot - (fc & (kTotFreq - 1));
+                        need = v < kRansL;
+                    }
+                    const uint32_t mask = __ballot_sync(0xffffffffu, need);
+                    if (need) {
+                        const uint64_t at = wp + 2 * __popc(mask & lt);
+                        v = (v << 16) | (uint32_t)p[at] | ((uint32_t)p[at + 1] << 8);
+                    }
+                    if (lane < 4) {
+                        out[i0 + lane] = (uint8_t)sy;
+                        xl = v;
+                    }
+                    wp += 2 * (uint64_t)__popc(mask);
+                    i0 += 4;
+                }
+                pos = wp - 16;  // the serial part below skips the states again
+            }
+        }
+        uint32_t xs4[4];
+        for (int k = 0; k < 4; k++) xs4[k] = __shfl_sync(0xffffffffu, xl, k);
         if (tid == 0) {
             if (status == FQXV_RANS_OK) {
                 uint32_t x[4];
-                for (int k = 0; k < 4; k++) x[k] = ld_u32_le(p + pos + 4 * k);
+                for (int k = 0; k < 4; k++) x[k] = xs4[k];
                 pos += 16;
                 uint8_t *out = dst + C.dst_off;
                 uint32_t ctx = 0;
-                for (uint64_t i = 0; i < n; i++) {
+                for (uint64_t i = i0; i < n; i++) {
                     const uint32_t t = ctxidx[ctx];
                     if (t == 0xffffu) {
                         status = FQXV_RANS_E_ABSENT_CONTEXT;
@@ -542,6 +618,23 @@ __global__ void __launch_bounds__(256) x_n4_decode_kernel(const uint8_t *__restr
         }
         __syncthreads();
     }
+}
+
+// The 4-state decoder's shared-memory limit, raised once per device.
+void ensure_n4_attr() {
+    static std::mutex mu;
+    static bool done[256];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+        cudaGetLastError();
+        return;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[dev]) return;
+    cudaFuncSetAttribute(x_n4_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kN4SmemRows * kN4Row));
+    cudaGetLastError();
+    done[dev] = true;
 }
 
 // Inverse RLE: literals + run bytes -> the array. One CTA per item, tiles of
@@ -720,8 +813,12 @@ int run_copies(fqxv_rans_ctx *ctx, XBufs &B, const uint8_t *src, uint8_t *dst, c
     CK(B.copies.ensure(cps.size() * sizeof(XCopy), s));
     CK(cudaStreamSynchronize(s));
     CK(cudaMemcpyAsync(B.copies.p, cps.data(), cps.size() * sizeof(XCopy), cudaMemcpyHostToDevice, s));
-    x_copy_kernel<<<(int)std::min<size_t>(cps.size(), (size_t)ctx->sms * 8), 256, 0, s>>>(
-        src, dst, B.copies.as<XCopy>(), (int)cps.size());
+    {
+        cudaEvent_t xt_ = ctx->timer.begin(s);
+        x_copy_kernel<<<(int)std::min<size_t>(cps.size(), (size_t)ctx->sms * 8), 256, 0, s>>>(
+            src, dst, B.copies.as<XCopy>(), (int)cps.size());
+        ctx->timer.end(kStXEncode, xt_, s);
+    }
     CK(cudaGetLastError());
     return FQXV_RANS_OK;
 }
@@ -777,12 +874,22 @@ int n4_encode(fqxv_rans_ctx *ctx, XBufs &B, const uint8_t *d_arena, const std::v
     CK(cudaMemcpyAsync(ctx->e_order.p, ord.data(), na * 4, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(B.misc.p, ooff.data(), na * 8, cudaMemcpyHostToDevice, s));
     EncBlock *dB = ctx->e_blocks.as<EncBlock>();
+    cudaEvent_t mt_ = ctx->timer.begin(s);
     CK(launch_enc_model(d_arena, dB, ctx->e_order.as<uint32_t>(), (int)na, ctx->e_tbl.as<uint8_t>(),
                         ctx->e_hist.as<uint32_t>(), nullptr, grid, 1, s));
-    x_n4_run_kernel<<<(int)((na + 127) / 128), 128, 0, s>>>(d_arena, dB, (int)na, ctx->e_tbl.as<uint8_t>(),
-                                                             ctx->e_words.as<uint16_t>());
-    x_n4_pack_kernel<<<grid, 256, 0, s>>>(dB, (int)na, ctx->e_tbl.as<uint8_t>(), ctx->e_words.as<uint16_t>(),
-                                           out.as<uint8_t>(), B.misc.as<uint64_t>());
+    ctx->timer.end(kStEncModel, mt_, s);
+    {
+        cudaEvent_t xt_ = ctx->timer.begin(s);
+        x_n4_run_kernel<<<(int)((na + 3) / 4), 128, 0, s>>>(d_arena, dB, (int)na, ctx->e_tbl.as<uint8_t>(),
+                                                                 ctx->e_words.as<uint16_t>());
+        ctx->timer.end(kStXEncode, xt_, s);
+    }
+    {
+        cudaEvent_t xt_ = ctx->timer.begin(s);
+        x_n4_pack_kernel<<<grid, 256, 0, s>>>(dB, (int)na, ctx->e_tbl.as<uint8_t>(), ctx->e_words.as<uint16_t>(),
+                                               out.as<uint8_t>(), B.misc.as<uint64_t>());
+        ctx->timer.end(kStXEncode, xt_, s);
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(hb.data(), dB, na * sizeof(EncBlock), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -845,7 +952,11 @@ int encode_flat(fqxv_rans_ctx *ctx, XBufs &B, const uint8_t *d_src, const std::v
     uint8_t *dW = B.work.as<uint8_t>();
     const int grid = (int)std::min<size_t>(ni, (size_t)ctx->sms * 4);
     if (pack) {
-        x_symset_kernel<<<grid, 256, 0, s>>>(d_src, dX, (int)ni);
+        {
+            cudaEvent_t xt_ = ctx->timer.begin(s);
+            x_symset_kernel<<<grid, 256, 0, s>>>(d_src, dX, (int)ni);
+            ctx->timer.end(kStXEncode, xt_, s);
+        }
         CK(cudaMemcpyAsync(hx.data(), dX, ni * sizeof(XItem), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         for (size_t i = 0; i < ni; i++) {
@@ -857,11 +968,23 @@ int encode_flat(fqxv_rans_ctx *ctx, XBufs &B, const uint8_t *d_src, const std::v
             X.m = (X.n * (uint64_t)pack_bits_h(X.nsym) + 7) / 8;
         }
         CK(cudaMemcpyAsync(dX, hx.data(), ni * sizeof(XItem), cudaMemcpyHostToDevice, s));
-        x_pack_kernel<<<grid, 256, 0, s>>>(d_src, dW, dX, (int)ni);
+        {
+            cudaEvent_t xt_ = ctx->timer.begin(s);
+            x_pack_kernel<<<grid, 256, 0, s>>>(d_src, dW, dX, (int)ni);
+            ctx->timer.end(kStXEncode, xt_, s);
+        }
     }
     if (rle) {
-        x_runsym_kernel<<<grid, 256, 0, s>>>(d_src, dW, dX, (int)ni);
-        x_rle_kernel<<<grid, kXThreads, 0, s>>>(d_src, dW, dX, (int)ni);
+        {
+            cudaEvent_t xt_ = ctx->timer.begin(s);
+            x_runsym_kernel<<<grid, 256, 0, s>>>(d_src, dW, dX, (int)ni);
+            ctx->timer.end(kStXEncode, xt_, s);
+        }
+        {
+            cudaEvent_t xt_ = ctx->timer.begin(s);
+            x_rle_kernel<<<grid, kXThreads, 0, s>>>(d_src, dW, dX, (int)ni);
+            ctx->timer.end(kStXEncode, xt_, s);
+        }
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(hx.data(), dX, ni * sizeof(XItem), cudaMemcpyDeviceToHost, s));
@@ -983,8 +1106,12 @@ int encode_stripe(fqxv_rans_ctx *ctx, XBufs &B, const uint8_t *d_src, const std:
     CK(cudaMemcpyAsync(dm, ioff.data(), ni * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(dm + ni, in.data(), ni * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(dm + 2 * ni, poff.data(), 4 * ni * 8, cudaMemcpyHostToDevice, s));
-    x_stripe_kernel<<<(int)std::min<size_t>(ni, (size_t)ctx->sms * 4), 256, 0, s>>>(d_src, B.planes.as<uint8_t>(), dm,
-                                                                                     dm + ni, dm + 2 * ni, (int)ni);
+    {
+        cudaEvent_t xt_ = ctx->timer.begin(s);
+        x_stripe_kernel<<<(int)std::min<size_t>(ni, (size_t)ctx->sms * 4), 256, 0, s>>>(d_src, B.planes.as<uint8_t>(), dm,
+                                                                                         dm + ni, dm + 2 * ni, (int)ni);
+        ctx->timer.end(kStXEncode, xt_, s);
+    }
     CK(cudaGetLastError());
     DevBuf nb;
     std::vector<Span> nres;
@@ -1149,8 +1276,12 @@ int gather_heads(fqxv_rans_ctx *ctx, XBufs &B, const uint8_t *d_src, const std::
     uint64_t *dm = B.misc.as<uint64_t>();
     CK(cudaMemcpyAsync(dm, off.data(), k * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(dm + k, len.data(), k * 8, cudaMemcpyHostToDevice, s));
-    x_head_kernel<<<(int)std::min<size_t>(k, (size_t)ctx->sms * 8), 128, 0, s>>>(d_src, dm, dm + k, (int)k,
-                                                                                 B.heads.as<uint8_t>());
+    {
+        cudaEvent_t xt_ = ctx->timer.begin(s);
+        x_head_kernel<<<(int)std::min<size_t>(k, (size_t)ctx->sms * 8), 128, 0, s>>>(d_src, dm, dm + k, (int)k,
+                                                                                     B.heads.as<uint8_t>());
+        ctx->timer.end(kStXDecode, xt_, s);
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out.data(), B.heads.p, k * kHead, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -1387,6 +1518,7 @@ int fqxv_rans_x_encode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqx
     st = run_copies(ctx, B, arena, d_dst, cps);
     if (st) return st;
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->timer.collect();
     return FQXV_RANS_OK;
 }
 
@@ -1531,6 +1663,7 @@ int fqxv_rans_x_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqx
     for (int ar = 0; ar < 3; ar++) {
         std::vector<XN4Dec> jobs;
         std::vector<size_t> who;
+        uint64_t kmax_all = 0;
         std::vector<XCopy> cps;
         uint64_t scr = 0;
         for (size_t k = 0; k < nodes.size(); k++) {
@@ -1555,6 +1688,7 @@ int fqxv_rans_x_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqx
                                               ? std::min<uint64_t>(256, N.core_len[c] > 41 ? (N.core_len[c] - 41) / 512 : 0)
                                               : 1;
                     scr += std::max<uint64_t>(kmax, 1) * kN4Row;
+                    kmax_all = std::max<uint64_t>(kmax_all, std::max<uint64_t>(kmax, 1));
                     jobs.push_back(J);
                     who.push_back(k * 2 + (size_t)c);
                 }
@@ -1567,8 +1701,15 @@ int fqxv_rans_x_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqx
         CK(B.items.ensure(jobs.size() * sizeof(XN4Dec), s));
         CK(cudaStreamSynchronize(s));
         CK(cudaMemcpyAsync(B.items.p, jobs.data(), jobs.size() * sizeof(XN4Dec), cudaMemcpyHostToDevice, s));
-        x_n4_decode_kernel<<<(int)std::min<size_t>(jobs.size(), (size_t)ctx->sms * 4), 256, 0, s>>>(
-            d_src, B.items.as<XN4Dec>(), (int)jobs.size(), B.core.as<uint8_t>(), arenas[ar]);
+        {
+            cudaEvent_t xt_ = ctx->timer.begin(s);
+            // rows of up to kN4SmemRows tables per core in shared memory
+            const int ksm = (int)std::min<uint64_t>(kmax_all, kN4SmemRows);
+            ensure_n4_attr();
+            x_n4_decode_kernel<<<(int)std::min<size_t>(jobs.size(), (size_t)ctx->sms * 4), 256, ksm * kN4Row, s>>>(
+                d_src, B.items.as<XN4Dec>(), (int)jobs.size(), B.core.as<uint8_t>(), arenas[ar], ksm);
+            ctx->timer.end(kStXDecode, xt_, s);
+        }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(jobs.data(), B.items.p, jobs.size() * sizeof(XN4Dec), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -1601,8 +1742,12 @@ int fqxv_rans_x_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqx
         if (!jobs.empty()) {
             CK(B.items.ensure(jobs.size() * sizeof(XUnrle), s));
             CK(cudaMemcpyAsync(B.items.p, jobs.data(), jobs.size() * sizeof(XUnrle), cudaMemcpyHostToDevice, s));
-            x_unrle_kernel<<<(int)std::min<size_t>(jobs.size(), (size_t)ctx->sms * 2), kXThreads, 0, s>>>(
-                B.work.as<uint8_t>(), B.items.as<XUnrle>(), (int)jobs.size(), B.vstart.as<uint64_t>());
+            {
+                cudaEvent_t xt_ = ctx->timer.begin(s);
+                x_unrle_kernel<<<(int)std::min<size_t>(jobs.size(), (size_t)ctx->sms * 2), kXThreads, 0, s>>>(
+                    B.work.as<uint8_t>(), B.items.as<XUnrle>(), (int)jobs.size(), B.vstart.as<uint64_t>());
+                ctx->timer.end(kStXDecode, xt_, s);
+            }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(jobs.data(), B.items.p, jobs.size() * sizeof(XUnrle), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
@@ -1636,8 +1781,12 @@ int fqxv_rans_x_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqx
         CK(B.items.ensure(jobs.size() * sizeof(XUnpack), s));
         CK(cudaStreamSynchronize(s));
         CK(cudaMemcpyAsync(B.items.p, jobs.data(), jobs.size() * sizeof(XUnpack), cudaMemcpyHostToDevice, s));
-        x_unpack_kernel<<<(int)std::min<size_t>(jobs.size(), (size_t)ctx->sms * 4), 256, 0, s>>>(
-            B.work.as<uint8_t>(), arenas[ar], B.items.as<XUnpack>(), (int)jobs.size());
+        {
+            cudaEvent_t xt_ = ctx->timer.begin(s);
+            x_unpack_kernel<<<(int)std::min<size_t>(jobs.size(), (size_t)ctx->sms * 4), 256, 0, s>>>(
+                B.work.as<uint8_t>(), arenas[ar], B.items.as<XUnpack>(), (int)jobs.size());
+            ctx->timer.end(kStXDecode, xt_, s);
+        }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(jobs.data(), B.items.p, jobs.size() * sizeof(XUnpack), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -1675,11 +1824,16 @@ int fqxv_rans_x_decode_batch(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqx
         CK(cudaMemcpyAsync(dm, oo.data(), k * 8, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(dm + k, on.data(), k * 8, cudaMemcpyHostToDevice, s));
         CK(cudaMemcpyAsync(dm + 2 * k, po.data(), 4 * k * 8, cudaMemcpyHostToDevice, s));
-        x_unstripe_kernel<<<(int)std::min<size_t>(k, (size_t)ctx->sms * 4), 256, 0, s>>>(
-            B.planes.as<uint8_t>(), arenas[lev == 0 ? 0 : 1], dm, dm + k, dm + 2 * k, (int)k);
+        {
+            cudaEvent_t xt_ = ctx->timer.begin(s);
+            x_unstripe_kernel<<<(int)std::min<size_t>(k, (size_t)ctx->sms * 4), 256, 0, s>>>(
+                B.planes.as<uint8_t>(), arenas[lev == 0 ? 0 : 1], dm, dm + k, dm + 2 * k, (int)k);
+            ctx->timer.end(kStXDecode, xt_, s);
+        }
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(s));
+    ctx->timer.collect();
     int first = FQXV_RANS_OK;
     for (size_t i = 0; i < nblocks; i++) {
         const XNode &N = nodes[i];
