@@ -232,6 +232,39 @@ def test_pinned_destination_mirror_unaligned(codec, orc):
     assert not pinned[:5].any() and not pinned[5 + total:].any()
 
 
+def test_host_pipeline_settings_change_no_byte(codec):
+    """The host-buffer pipeline choices (input read in place or copied, output
+    mirrored by the decoding CTAs or copied after the batch, chunk counts)
+    give the same streams and the same decoded bytes."""
+    import torch
+
+    data, spans, _ = W.config2(nblocks=700, lo=1000, hi=400_000, seed=55)
+    assert len(data) >= (32 << 20)  # large enough to be cut into chunks
+    h_src = torch.from_numpy(data.copy()).pin_memory().numpy()
+    bound = codec.encode_bound(spans, 2)
+    ref = None
+    keys = ("host_enc_chunks", "host_dec_chunks", "host_in_place", "host_out_mirror")
+    old = {k: codec.get_param(k) for k in keys}
+    try:
+        for enc_chunks, dec_chunks, in_place, mirror in ((1, 1, -1, 1), (4, 4, 0, 0), (2, 1, 1, 1), (8, 2, 1, 0)):
+            codec.set_param("host_enc_chunks", enc_chunks)
+            codec.set_param("host_dec_chunks", dec_chunks)
+            codec.set_param("host_in_place", in_place)
+            codec.set_param("host_out_mirror", mirror)
+            h_enc = torch.zeros(bound, dtype=torch.uint8).pin_memory().numpy()
+            es, _ = codec.encode_batch_host(h_src, spans, 2, h_enc)
+            total = int(es[-1, 0] + es[-1, 1])
+            if ref is None:
+                ref = (es.copy(), h_enc[:total].copy())
+            assert np.array_equal(es, ref[0]) and np.array_equal(h_enc[:total], ref[1])
+            h_dec = torch.zeros(len(data), dtype=torch.uint8).pin_memory().numpy()
+            lens, st = codec.decode_batch_host(h_enc, es, spans, h_dec)
+            assert (st == 0).all() and np.array_equal(h_dec, data)
+    finally:
+        for k, v in old.items():
+            codec.set_param(k, v)
+
+
 def test_small_alphabet_order1_statuses_match_oracle(codec, orc):
     """Order-1 streams of small alphabets (the one-warp decoder): good,
     truncated and corrupted streams give the oracle's bytes and statuses."""
