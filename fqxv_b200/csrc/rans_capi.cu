@@ -357,7 +357,9 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             smem[g] = dec_smem_bytes(gcls[g], gcls[g] == kClsO1Dense ? tmaxp[g] : tmax[g], ndmax[g]);
             // the groups of largest streams: one CTA per SM, alone on it
             if ((g == kGroupFourTop || g == kGroupSmallTop) && ctx->tune.o1_top_exclusive)
-                smem[g] = std::max(smem[g], dec_exclusive_smem(gcls[g]));
+                smem[g] = std::max(smem[g], dec_exclusive_smem(gcls[g], g == kGroupSmallTop
+                                                                              ? (int)ctx->tune.o1_top_small_per_sm
+                                                                              : 1));
         }
         // Groups are launched longest first -- by the serial time of their
         // largest stream (rounds x cycles per round: ~620 for order-1,

@@ -112,6 +112,9 @@ struct Tuning {
     // (their CTAs claim the SM's shared memory), so their serial chains are
     // not slowed by the rest of the batch; 0: they share.
     int64_t o1_top_exclusive = 1;
+    // CTAs per SM of the small-alphabet top group when exclusive: each is one
+    // warp, so up to four can hold an SM together, one per scheduler.
+    int64_t o1_top_small_per_sm = 4;
     // CTAs per SM of each decode class, at most (the occupancy API bounds it too)
     int64_t cta_cap_o0 = 32, cta_cap_o1_small = 32, cta_cap_o1_wide = 32, cta_cap_o1_four = 8,
             cta_cap_o1_global = 32;

@@ -1469,21 +1469,27 @@ uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes, int nd) {
 
 // Dynamic shared memory of one CTA that leaves no room on its SM for any
 // other: the per-block opt-in maximum less the kernel's static shared memory.
-static uint32_t exclusive_bytes(const void *fn) {
-    int dev = 0, optin = 0;
+// With per_sm > 1: the share that lets exactly per_sm such CTAs fill an SM
+// (each CTA also costs its static shared memory and the 1 KB the driver
+// reserves per block).
+static uint32_t exclusive_bytes(const void *fn, int per_sm) {
+    int dev = 0, optin = 0, per_smem = 0;
     cudaFuncAttributes a;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&per_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
         cudaFuncGetAttributes(&a, fn) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    return optin > (int)a.sharedSizeBytes ? (uint32_t)(optin - (int)a.sharedSizeBytes) / 128 * 128 : 0u;
+    int64_t b = (int64_t)optin - (int64_t)a.sharedSizeBytes;
+    if (per_sm > 1) b = std::min<int64_t>(b, (int64_t)per_smem / per_sm - 1024 - (int64_t)a.sharedSizeBytes);
+    return b > 0 ? (uint32_t)b / 128 * 128 : 0u;
 }
 
-uint32_t dec_exclusive_smem(int cls) {
-    if (cls == kClsO1Dense) return exclusive_bytes(reinterpret_cast<const void *>(dec_o1d_kernel));
-    if (cls == kClsO1Small) return exclusive_bytes(reinterpret_cast<const void *>(dec_o1w_kernel<false>));
+uint32_t dec_exclusive_smem(int cls, int per_sm) {
+    if (cls == kClsO1Dense) return exclusive_bytes(reinterpret_cast<const void *>(dec_o1d_kernel), per_sm);
+    if (cls == kClsO1Small) return exclusive_bytes(reinterpret_cast<const void *>(dec_o1w_kernel<false>), per_sm);
     return 0;
 }
 

@@ -220,7 +220,8 @@ uint32_t dec_smem_bytes(int cls, uint32_t tbl_bytes, int nd = kDenseMax);
 __host__ __device__ inline uint32_t wide_rows_bytes(int nd) { return (uint32_t)((2 * (3 * nd + 2) * 16 + 127) / 128 * 128); }
 // Dynamic shared memory with which one CTA of a decode class fills an SM (no
 // other CTA fits beside it); 0 when the class cannot.
-uint32_t dec_exclusive_smem(int cls);
+// per_sm > 1: the share that lets exactly per_sm such CTAs fill an SM.
+uint32_t dec_exclusive_smem(int cls, int per_sm = 1);
 // CTAs of a decode class that fit on one SM with `smem_bytes` of dynamic
 // shared memory (registers and static shared memory included).
 int dec_blocks_per_sm(int cls, uint32_t smem_bytes);

@@ -37,6 +37,7 @@ const ParamDef kParams[] = {
     {"o1_top_latency_pct", &Tuning::o1_top_latency_pct, 0, 100000},
     {"o1_top_max", &Tuning::o1_top_max, -1, 1 << 30},
     {"o1_top_exclusive", &Tuning::o1_top_exclusive, 0, 1},
+    {"o1_top_small_per_sm", &Tuning::o1_top_small_per_sm, 1, 4},
     {"cta_cap_o0", &Tuning::cta_cap_o0, 1, 64},
     {"cta_cap_o1_small", &Tuning::cta_cap_o1_small, 1, 64},
     {"cta_cap_o1_wide", &Tuning::cta_cap_o1_wide, 1, 64},

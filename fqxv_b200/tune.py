@@ -16,7 +16,8 @@ reference's only run-time choice is its SIMD backend
                         four-warp decoder, small ones on the one-warp one)
   o1_top_max            at most this many streams (the longest) in those
                         groups
-  o1_top_exclusive      1: those two groups run one CTA per SM alone on it
+  o1_top_exclusive      1: those two groups run on SMs of their own
+  o1_top_small_per_sm   CTAs (one warp each) per such SM of the small group
   enc_o1_keys           order-1 encode reads per-position table indices stored
                         by the model kernel (1) or derives them (0)
   o1_four_max_streams   below this many wide-alphabet order-1 streams in a
@@ -47,7 +48,7 @@ from . import workloads as W
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 # the library's built-in rules (csrc/rans_ctx.cuh, struct Tuning)
-DEFAULTS = {"o1_four_max_streams": -1, "o1_top_latency_pct": 75, "o1_top_max": -1, "o1_top_exclusive": 1, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
+DEFAULTS = {"o1_four_max_streams": -1, "o1_top_latency_pct": 75, "o1_top_max": -1, "o1_top_exclusive": 1, "o1_top_small_per_sm": 4, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
             "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "dense_edge_small": 40 << 10,
             "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 16, "enc_o1_keys": 1}
 
@@ -159,6 +160,7 @@ def sweep(reps: int = 3) -> dict:
     pick("o1_top_exclusive", (1, 0), score)
     pick("o1_top_latency_pct", (25, 50, 75, 100, 150, 100000), score)
     pick("o1_top_max", (sms // 4, sms // 2, 3 * sms // 4, sms), score)
+    pick("o1_top_small_per_sm", (1, 2, 4), score)
     pick("o1_four_max_streams", (0, sms // 2, sms, 2 * sms, 4 * sms, 1 << 30), score)
 
     # CTAs per SM on batches of the peak-throughput shape (2048 x 512 KiB):

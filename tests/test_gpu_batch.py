@@ -356,6 +356,7 @@ def test_launch_shapes_change_no_byte(codec):
          "dense_edge_large": 160 << 10},
         {"o1_top_exclusive": 0, "o1_top_max": 0, "enc_o1_keys": 0},
         {"o1_top_exclusive": 1, "o1_top_max": 5, "o1_top_latency_pct": 0},
+        {"o1_top_exclusive": 1, "o1_top_max": 9, "o1_top_latency_pct": 0, "o1_top_small_per_sm": 2},
         {"o1_top_exclusive": 1, "o1_top_max": 1 << 20, "o1_top_latency_pct": 0, "enc_o1_keys": 0},
     ]
     defaults = {k: codec.get_param(k) for s in settings for k in s}

@@ -13,6 +13,7 @@ KNOWN = {
     "o1_top_latency_pct": (0, 100000),
     "o1_top_max": (-1, 1 << 30),
     "o1_top_exclusive": (0, 1),
+    "o1_top_small_per_sm": (1, 4),
     "cta_cap_o0": (1, 64),
     "cta_cap_o1_small": (1, 64),
     "cta_cap_o1_wide": (1, 64),
