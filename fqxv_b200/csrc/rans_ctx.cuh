@@ -122,7 +122,7 @@ struct Tuning {
     // launch groups (a launch's shared memory is its largest member's)
     int64_t dense_edge_small = 40 << 10, dense_edge_large = 80 << 10;
     // encode kernel grid, CTAs per SM
-    int64_t enc_run_ctas_per_sm = 16;
+    int64_t enc_run_ctas_per_sm = 2;
     // Order-1 encode: 1, the model kernel stores each position's table index
     // (u16) for the encode kernel to read back; 0, the encode kernel derives
     // it from the byte and its predecessor (no per-position array).
