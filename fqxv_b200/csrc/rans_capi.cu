@@ -395,9 +395,15 @@ int decode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
             CK(cudaStreamWaitEvent(as, ctx->ev_fork, 0));
             int per_sm = dec_blocks_per_sm(cls, smem[g]);
             const Tuning &T = ctx->tune;
-            const int64_t cap = cls == kClsO0 ? T.cta_cap_o0 : cls == kClsO1Small ? T.cta_cap_o1_small
-                                : cls == kClsO1Wide ? T.cta_cap_o1_wide : cls == kClsO1Dense ? T.cta_cap_o1_four
-                                                                                            : T.cta_cap_o1_global;
+            int64_t cap = cls == kClsO0 ? T.cta_cap_o0 : cls == kClsO1Small ? T.cta_cap_o1_small
+                          : cls == kClsO1Wide ? T.cta_cap_o1_wide : cls == kClsO1Dense ? T.cta_cap_o1_four
+                                                                                      : T.cta_cap_o1_global;
+            // A batch bound by its top groups only needs the rest done by
+            // then: fewer one-warp CTAs per SM slow its largest streams less.
+            if (ntop && g != kGroupSmallTop && g != kGroupFourTop) {
+                if (cls == kClsO1Small) cap = std::min<int64_t>(cap, T.cta_cap_o1_small_topped);
+                if (cls == kClsO1Wide) cap = std::min<int64_t>(cap, T.cta_cap_o1_wide_topped);
+            }
             per_sm = std::max(1, std::min<int>(per_sm, (int)cap));
             ctx->timer.shape(stage, per_sm, smem[g]);
             if (persistent) {

@@ -118,6 +118,9 @@ struct Tuning {
     // CTAs per SM of each decode class, at most (the occupancy API bounds it too)
     int64_t cta_cap_o0 = 32, cta_cap_o1_small = 32, cta_cap_o1_wide = 32, cta_cap_o1_four = 8,
             cta_cap_o1_global = 32;
+    // the same for the one-warp classes outside the top groups when a batch
+    // has top groups
+    int64_t cta_cap_o1_small_topped = 4, cta_cap_o1_wide_topped = 3;
     // table-image sizes cutting the other dense wide-alphabet streams into
     // launch groups (a launch's shared memory is its largest member's)
     int64_t dense_edge_small = 40 << 10, dense_edge_large = 80 << 10;

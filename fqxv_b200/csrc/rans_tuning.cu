@@ -43,6 +43,8 @@ const ParamDef kParams[] = {
     {"cta_cap_o1_wide", &Tuning::cta_cap_o1_wide, 1, 64},
     {"cta_cap_o1_four", &Tuning::cta_cap_o1_four, 1, 16},
     {"cta_cap_o1_global", &Tuning::cta_cap_o1_global, 1, 64},
+    {"cta_cap_o1_small_topped", &Tuning::cta_cap_o1_small_topped, 1, 64},
+    {"cta_cap_o1_wide_topped", &Tuning::cta_cap_o1_wide_topped, 1, 64},
     {"dense_edge_small", &Tuning::dense_edge_small, 0, kDenseImageMax},
     {"dense_edge_large", &Tuning::dense_edge_large, 0, kDenseImageMax},
     {"enc_run_ctas_per_sm", &Tuning::enc_run_ctas_per_sm, 1, 64},

@@ -24,6 +24,9 @@ reference's only run-time choice is its SIMD backend
                         launch group the four-warp decoder (one stream per
                         SM, lower latency per stream) runs them, else the
                         one-warp decoder (several streams per SM)
+  cta_cap_o1_small_topped / cta_cap_o1_wide_topped
+                        the same outside the top groups of a batch that has
+                        them (its largest bulk streams run less contended)
   cta_cap_o0 / cta_cap_o1_small / cta_cap_o1_wide / cta_cap_o1_global
                         CTAs per SM of each decode class (the occupancy
                         API's figure is the upper bound)
@@ -49,7 +52,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 # the library's built-in rules (csrc/rans_ctx.cuh, struct Tuning)
 DEFAULTS = {"o1_four_max_streams": -1, "o1_top_latency_pct": 75, "o1_top_max": -1, "o1_top_exclusive": 1, "o1_top_small_per_sm": 4, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
-            "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "dense_edge_small": 40 << 10,
+            "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "cta_cap_o1_small_topped": 4,
+            "cta_cap_o1_wide_topped": 3, "dense_edge_small": 40 << 10,
             "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 2, "enc_o1_keys": 1}
 
 
@@ -162,6 +166,9 @@ def sweep(reps: int = 3) -> dict:
     pick("o1_top_max", (sms // 4, sms // 2, 3 * sms // 4, sms), score)
     pick("o1_top_small_per_sm", (1, 2, 4), score)
     pick("o1_four_max_streams", (0, sms // 2, sms, 2 * sms, 4 * sms, 1 << 30), score)
+    # one-warp CTAs per SM outside the top groups, when a batch has them
+    pick("cta_cap_o1_small_topped", (2, 4, 8, 16), lambda: bm.decode_gbs(reps))
+    pick("cta_cap_o1_wide_topped", (2, 3, 4, 6), lambda: bm.decode_gbs(reps))
 
     # CTAs per SM on batches of the peak-throughput shape (2048 x 512 KiB):
     # enough streams that every cap fills the GPU several times over

@@ -19,6 +19,8 @@ KNOWN = {
     "cta_cap_o1_wide": (1, 64),
     "cta_cap_o1_four": (1, 16),
     "cta_cap_o1_global": (1, 64),
+    "cta_cap_o1_small_topped": (1, 64),
+    "cta_cap_o1_wide_topped": (1, 64),
     "dense_edge_small": (0, 160 * 1024),
     "dense_edge_large": (0, 160 * 1024),
     "enc_run_ctas_per_sm": (1, 64),
