@@ -275,6 +275,11 @@ int fqxv_rans_server_create(int device, int n_workers, uint64_t hbm_cap, fqxv_ra
             delete s;
             return st;
         }
+        // Workers decode their batches side by side on one GPU: a batch's
+        // top groups must not claim SMs of their own there, or each worker's
+        // CTAs wait for SMs the others hold (config4's capacity, measured on
+        // B200: 0.16-0.18 GB/s with them, 0.23-0.29 without).
+        fqxv_rans_ctx_set_param(c, "o1_top_exclusive", 0);
         s->ctxs.push_back(c);
     }
     for (int i = 0; i < n_workers; i++) s->workers.emplace_back([s, i] { s->worker(i); });
