@@ -37,8 +37,8 @@ uint64_t enc_bound_one(uint64_t n, int order) {
     return kHdr + tables + kStatesBytes + 2 * n;
 }
 
-// Smallest batch output written in place into a pinned host destination,
-// and fewest streams whose pinned input is read in place.
+// Smallest batch output mirrored into a pinned host destination by the
+// decoding CTAs, and fewest streams whose pinned input is read in place.
 constexpr uint64_t kZeroCopyMinBytes = 4ull << 20;
 constexpr size_t kZeroCopyMinStreams = 256;
 

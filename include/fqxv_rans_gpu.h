@@ -237,21 +237,22 @@ int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int order, uint8_t 
 
 /* ---- launch shapes -------------------------------------------------------
  * No reference counterpart beyond Backend::detect (lib.rs:80-97). Every
- * context has integer launch-shape parameters (decoder choice for wide
+ * context has integer launch-shape parameters: the decoder choice for wide
  * order-1 alphabets by stream count, the launch groups of the order-1
  * streams that bound a batch, CTAs per SM of each decode class, dense-table
- * group edges, encode grid, order-1 key array, host-buffer pipeline); they
- * start from the tuning
- * table of the device when
- * one is found (FQXV_RANS_TUNING, else tuning/<device>.json beside the
- * package directory of the library), else from the built-in rules. Names:
- * o1_four_max_streams, o1_top_latency_pct, o1_top_max, o1_top_exclusive, o1_top_small_per_sm,
- * cta_cap_o0, cta_cap_o1_small, cta_cap_o1_wide, cta_cap_o1_four,
- * cta_cap_o1_global, cta_cap_o1_small_topped, cta_cap_o1_wide_topped, dense_edge_small, dense_edge_large, enc_run_ctas_per_sm,
- * enc_o1_keys, host_enc_chunks, host_dec_chunks, host_in_place, host_out_mirror.
- * Unknown names and
- * out-of-range values: FQXV_RANS_E_INVALID_ARG. Output bytes never depend on
- * them. */
+ * group edges, the encode grid, the order-1 key array and the host-buffer
+ * pipeline. They start from the tuning table of the device when one is found
+ * (FQXV_RANS_TUNING, else tuning/<device>.json beside the package directory
+ * of the library), else from the built-in rules. Names:
+ *   o1_four_max_streams, o1_top_latency_pct, o1_top_max, o1_top_exclusive,
+ *   o1_top_small_per_sm,
+ *   cta_cap_o0, cta_cap_o1_small, cta_cap_o1_wide, cta_cap_o1_four,
+ *   cta_cap_o1_global, cta_cap_o1_small_topped, cta_cap_o1_wide_topped,
+ *   dense_edge_small, dense_edge_large,
+ *   enc_run_ctas_per_sm, enc_o1_keys,
+ *   host_enc_chunks, host_dec_chunks, host_in_place, host_out_mirror.
+ * Unknown names and out-of-range values: FQXV_RANS_E_INVALID_ARG. Output
+ * bytes never depend on them. */
 int fqxv_rans_ctx_set_param(fqxv_rans_ctx *ctx, const char *name, int64_t value);
 int fqxv_rans_ctx_get_param(fqxv_rans_ctx *ctx, const char *name, int64_t *value);
 /* Path of the tuning table the context applied ("" when none). */
