@@ -162,3 +162,21 @@ def test_truncated_streams_match_the_definition(codec, orc):
     _, lens, st = codec.x_decode_batch(_dev(arena), spans, rsp, raise_on_error=False)
     want = [orc.x_decode_status(s, c) for s, c in zip(streams, caps)]
     assert list(st) == want
+
+
+@pytest.mark.parametrize("flags", [0x02, 0x03])
+def test_four_way_cores_ragged_lengths(codec, orc, flags):
+    """4-way cores whose length is not a multiple of four, and long enough
+    that the decoder's four-lane rounds run before the serial remainder:
+    the GPU streams equal the definition's and decode back."""
+    blobs = [W.binned_quality(n, 700 + n % 7).tobytes() for n in (4, 5, 6, 7, 8001, 8002, 8003, 65537, 100_003)]
+    blobs += [W.full_quality(n, 710 + n % 5).tobytes() for n in (9, 70_001, 131_075)]
+    streams = _check_encode(codec, orc, blobs, flags)
+    arena, spans = _arena(streams)
+    _, ospans = _arena(blobs)
+    d_dec, lens, st = codec.x_decode_batch(_dev(arena), spans, ospans)
+    dec = d_dec.cpu().numpy()
+    for i, b in enumerate(blobs):
+        assert st[i] == 0 and int(lens[i]) == len(b)
+        o = int(ospans[i, 0])
+        assert dec[o:o + len(b)].tobytes() == b, i
