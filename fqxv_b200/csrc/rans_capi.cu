@@ -146,7 +146,17 @@ int encode_batch_impl(fqxv_rans_ctx *ctx, const uint8_t *d_src, const fqxv_rans_
     uint8_t *dT = ctx->e_tbl.as<uint8_t>();
     uint16_t *dW = ctx->e_words.as<uint16_t>();
     uint32_t *dH = ctx->e_hist.as<uint32_t>();
-    const int run_grid = ctx->sms * (int)ctx->tune.enc_run_ctas_per_sm;
+    // A batch whose largest block is far above its mean has a serial tail:
+    // its largest jobs run faster with fewer warps per scheduler
+    // (enc_run_ctas_per_sm). A batch of like-sized blocks is throughput-bound
+    // and takes enc_run_ctas_per_sm_uniform.
+    uint64_t nsum = 0, nmax = 0;
+    for (size_t i = 0; i < nb; i++) {
+        nsum += hb[i].n;
+        nmax = std::max<uint64_t>(nmax, hb[i].n);
+    }
+    const bool tail = (double)nmax > 4.0 * (double)nsum / (double)nb;
+    const int run_grid = ctx->sms * (int)(tail ? ctx->tune.enc_run_ctas_per_sm : ctx->tune.enc_run_ctas_per_sm_uniform);
     if (persistent) {
         cudaEvent_t t0;
         if (nlarge) {

@@ -126,6 +126,9 @@ struct Tuning {
     int64_t dense_edge_small = 40 << 10, dense_edge_large = 80 << 10;
     // encode kernel grid, CTAs per SM
     int64_t enc_run_ctas_per_sm = 2;
+    // the same for batches of like-sized blocks (no block above four times
+    // the mean)
+    int64_t enc_run_ctas_per_sm_uniform = 3;
     // Order-1 encode: 1, the model kernel stores each position's table index
     // (u16) for the encode kernel to read back; 0, the encode kernel derives
     // it from the byte and its predecessor (no per-position array).

@@ -48,6 +48,7 @@ const ParamDef kParams[] = {
     {"dense_edge_small", &Tuning::dense_edge_small, 0, kDenseImageMax},
     {"dense_edge_large", &Tuning::dense_edge_large, 0, kDenseImageMax},
     {"enc_run_ctas_per_sm", &Tuning::enc_run_ctas_per_sm, 1, 64},
+    {"enc_run_ctas_per_sm_uniform", &Tuning::enc_run_ctas_per_sm_uniform, 1, 64},
     {"enc_o1_keys", &Tuning::enc_o1_keys, 0, 1},
     {"host_enc_chunks", &Tuning::host_enc_chunks, 1, 16},
     {"host_dec_chunks", &Tuning::host_dec_chunks, 1, 16},

@@ -54,7 +54,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULTS = {"o1_four_max_streams": -1, "o1_top_latency_pct": 75, "o1_top_max": -1, "o1_top_exclusive": 1, "o1_top_small_per_sm": 4, "cta_cap_o0": 32, "cta_cap_o1_small": 32, "cta_cap_o1_wide": 32,
             "cta_cap_o1_four": 8, "cta_cap_o1_global": 32, "cta_cap_o1_small_topped": 4,
             "cta_cap_o1_wide_topped": 3, "dense_edge_small": 40 << 10,
-            "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 2, "enc_o1_keys": 1}
+            "dense_edge_large": 80 << 10, "enc_run_ctas_per_sm": 2, "enc_run_ctas_per_sm_uniform": 3, "enc_o1_keys": 1}
 
 
 def _batch(kind: str, nblocks: int, block: int, seed: int):

@@ -249,7 +249,7 @@ int fqxv_rans_encode_noalloc(const uint8_t *d_src, size_t n, int order, uint8_t 
  *   cta_cap_o0, cta_cap_o1_small, cta_cap_o1_wide, cta_cap_o1_four,
  *   cta_cap_o1_global, cta_cap_o1_small_topped, cta_cap_o1_wide_topped,
  *   dense_edge_small, dense_edge_large,
- *   enc_run_ctas_per_sm, enc_o1_keys,
+ *   enc_run_ctas_per_sm, enc_run_ctas_per_sm_uniform, enc_o1_keys,
  *   host_enc_chunks, host_dec_chunks, host_in_place, host_out_mirror.
  * Unknown names and out-of-range values: FQXV_RANS_E_INVALID_ARG. Output
  * bytes never depend on them. */

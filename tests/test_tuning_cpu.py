@@ -24,6 +24,7 @@ KNOWN = {
     "dense_edge_small": (0, 160 * 1024),
     "dense_edge_large": (0, 160 * 1024),
     "enc_run_ctas_per_sm": (1, 64),
+    "enc_run_ctas_per_sm_uniform": (1, 64),
     "enc_o1_keys": (0, 1),
     "host_enc_chunks": (1, 16),
     "host_dec_chunks": (1, 16),
